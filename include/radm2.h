@@ -1,0 +1,202 @@
+/*
+ * radm2.h -- C ABI of the B200 batched RADM2 Rosenbrock (ROS-3) chemistry solver.
+ *
+ * Drop-in for the reference's host path (Rizkyanno/RADM2-Solver-Multi-GPU, mgpu.cu):
+ * the reference keeps its per-cell arrays in library-owned device globals, fills
+ * them with dev_convert, computes rate constants with updatingCoefficientWRFChemData()
+ * and integrates every cell with Rosenbrock(Tstart, Tend, AbsTol, RelTol, RPAR, IPAR).
+ * Here the device arrays live in a context; the same three steps are
+ * radm2_set_inputs, radm2_update_rconst and radm2_rosenbrock, with the reference's
+ * argument meaning, IPAR/RPAR conventions and IERR codes.
+ *
+ * Conventions: every function returns RADM2_OK (0) or a negative RADM2_E* code,
+ * except radm2_rosenbrock / radm2_run_split, which return the reference's IERR
+ * (1 = success, -1..-8 = Rosenbrock error, see radm2_error_string) or a RADM2_E*
+ * code (<= -100) for API/CUDA failures.  No function prints or exits.  A context
+ * is used by one host thread at a time; different contexts are independent.
+ * Host arrays are in the reference's per-cell (array-of-structs) layout; the
+ * library keeps struct-of-arrays copies in device memory.
+ */
+#ifndef RADM2_H
+#define RADM2_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RADM2_NVAR 59        /* variable species (mgpu.cu:18) */
+#define RADM2_NFIX 2         /* fixed species: [0] H2O, [1] M (mgpu.cu:20, 191-192) */
+#define RADM2_NREACT 156     /* reactions / rate constants (mgpu.cu:21) */
+#define RADM2_NPH 28         /* photolysis rates per cell (mgpu.cu:48) */
+#define RADM2_LU_NONZERO 659 /* LU slots (mgpu.cu:25) */
+
+/* API / runtime error codes (Rosenbrock's own IERR codes are -1..-8). */
+#define RADM2_OK 0
+#define RADM2_E_ARG (-100)      /* bad argument (null pointer, size, option) */
+#define RADM2_E_CUDA (-101)     /* CUDA runtime error; radm2_last_error has the text */
+#define RADM2_E_NOMEM (-102)    /* device allocation failed */
+#define RADM2_E_STATE (-103)    /* call out of order (e.g. rosenbrock before set_inputs) */
+#define RADM2_E_NODEV (-104)    /* no usable sm_100 device */
+#define RADM2_E_TOOBIG (-105)   /* size exceeds a documented maximum */
+
+/* Solver variants. */
+#define RADM2_PREC_FP64 0    /* plain FP64 method (reference parity) */
+#define RADM2_PREC_FP32LU 1  /* FP32 Jacobian/LU + FP64 iterative refinement; FP64 state */
+
+#define RADM2_SCHED_STATIC 0     /* one thread per cell, cells in order (plain) */
+#define RADM2_SCHED_PERSISTENT 1 /* persistent grid, per-lane work stealing */
+
+typedef struct radm2_opts {
+    int device;         /* CUDA device ordinal (default 0) */
+    int precision;      /* RADM2_PREC_* (default FP64) */
+    int refine_sweeps;  /* FP32LU: FP64 refinement sweeps per stage solve, 0..2 (default 1) */
+    int schedule;       /* RADM2_SCHED_* (default STATIC) */
+    int block_threads;  /* threads per block: 0 = default (128); 64, 128 or 256 */
+    int blocks_per_sm;  /* persistent grid blocks per SM: 0 = default */
+    int float_coeffs;   /* 1 (default): M/E rounded through float as mgpu.cu:3300-3304 */
+    int placement;      /* working-set placement: RADM2_PLACE_* (default GLOBAL) */
+    int min_blocks;     /* register cap for occupancy: build variant with at least this many
+                           resident blocks per SM (0/1 = no cap; 3 or 4 with 128 threads) */
+} radm2_opts;
+
+/* Placement of each thread's working set (rate constants + state, and the LU). */
+#define RADM2_PLACE_GLOBAL 0   /* all in the thread's global scratch slot */
+#define RADM2_PLACE_LU_SMEM 1  /* LU in shared memory (32 or 64 threads per block) */
+#define RADM2_PLACE_ALL_SMEM 3 /* LU, rate constants and state in shared memory (32 threads) */
+
+typedef struct radm2_ctx radm2_ctx;
+
+/* Aggregates of the last integration (also folded into IPAR/RPAR). */
+typedef struct radm2_stats {
+    long long n_accepted;  /* accepted steps, summed over cells */
+    long long n_rejected;  /* rejected steps, summed over cells */
+    long long n_failed;    /* cells that ended with a negative status */
+    int worst_status;      /* minimum per-cell status (1 = all ok) */
+    int max_steps_cell;    /* largest per-cell accepted+rejected count */
+    double texit_min;      /* least advanced exit time */
+    double hexit_min;      /* smallest step proposed at exit */
+} radm2_stats;
+
+/* Fill opts with the defaults above. */
+int radm2_opts_default(radm2_opts *opts);
+
+/* Create a context on opts->device (opts may be NULL for defaults). */
+int radm2_create(radm2_ctx **ctx, const radm2_opts *opts);
+int radm2_destroy(radm2_ctx *ctx);
+
+/* Human-readable text for an IERR (-1..-8, the messages of ros_ErrorMsg,
+ * mgpu.cu:976-1005) or a RADM2_E* code. */
+const char *radm2_error_string(int code);
+/* Text of the last CUDA/API failure on this context. */
+const char *radm2_last_error(const radm2_ctx *ctx);
+
+/* Use the caller's cudaStream_t for all work of this context (NULL = the context's own). */
+int radm2_set_stream(radm2_ctx *ctx, void *cuda_stream);
+int radm2_synchronize(radm2_ctx *ctx);
+
+/*
+ * Per-cell inputs, host pointers, reference layout.  Replaces the device arrays
+ * dev_convert writes (mgpu.cu:513-646): VAR[ncell][59] species (molec/cm^3),
+ * FIX[ncell][2] = {H2O, M}, TEMP[ncell] (K), RC_N2O5[ncell] (N2O5 + H2O rate; NULL
+ * = zero, which is what mgpu.cu:552's formula evaluates to), JV[ncell][28]
+ * photolysis rates (1/s).  Copies to the device (stream-ordered; host buffers
+ * may be reused once the call returns).
+ */
+int radm2_set_inputs(radm2_ctx *ctx, int ncell, const double *VAR, const double *FIX, const double *TEMP,
+                     const double *RC_N2O5, const double *JV);
+
+/* Species state only (VAR[ncell][59]); the cell count must match set_inputs. */
+int radm2_set_state(radm2_ctx *ctx, const double *VAR);
+int radm2_get_state(radm2_ctx *ctx, double *VAR);
+
+/* Same inputs, already in device memory in struct-of-arrays layout:
+ * var[59][ld], fix[2][ld], temp[ld], rc_n2o5[ld] (NULL = zero), jv[28][ld], with
+ * ld >= ncell the leading dimension.  Device-to-device copy. */
+int radm2_set_inputs_device(radm2_ctx *ctx, int ncell, int ld, const double *var, const double *fix,
+                            const double *temp, const double *rc_n2o5, const double *jv);
+int radm2_get_state_device(radm2_ctx *ctx, double *var, int ld);
+/* Species state only, from device memory var[59][ld] (device-to-device). */
+int radm2_set_state_device(radm2_ctx *ctx, const double *var, int ld);
+
+/* Rate constants for every cell, replaces updatingCoefficientWRFChemData()
+ * (mgpu.cu:921-947; kernel dev_Update_RCONST, mgpu.cu:752-919). */
+int radm2_update_rconst(radm2_ctx *ctx);
+/* Copy the rate constants out, RCONST[ncell][156] (host). */
+int radm2_get_rconst(radm2_ctx *ctx, double *RCONST);
+/* Override the rate constants with caller values, RCONST[ncell][156] (host). */
+int radm2_set_rconst(radm2_ctx *ctx, const double *RCONST);
+
+/*
+ * Integrate every cell from Tstart to Tend.  Replaces Rosenbrock() (mgpu.cu:3664-3848):
+ * same IPAR/RPAR meaning and validation (IPAR[0] autonomous, IPAR[1] scalar tol,
+ * IPAR[2] max steps, IPAR[3]=2 ROS-3; RPAR[0..6] Hmin, Hmax, Hstart, FacMin, FacMax,
+ * FacRej, FacSafe), same return codes.  Counters are accumulated into IPAR[10..17]
+ * (Nfun, Njac, Nstp, Nacc, Nrej, Ndec, Nsol, Nsng), summed over cells;
+ * RPAR[10] = Texit of the least advanced cell, RPAR[11] = smallest exit step.
+ * Each cell runs its own step-size loop on the device; the call blocks until done.
+ */
+int radm2_rosenbrock(radm2_ctx *ctx, double Tstart, double Tend, const double *AbsTol, const double *RelTol,
+                     double *RPAR, int *IPAR);
+
+/* Operator-split loop: nsplit back-to-back integrations of [0, dt], the state
+ * carried over, replayed as one CUDA graph when use_graph != 0.  IPAR/RPAR as
+ * for radm2_rosenbrock (RPAR[2] = 0 means Hstart = 0.01*dt, the reference
+ * driver's ratio, mgpu.cu:3873).  Returns IERR of the worst split. */
+int radm2_run_split(radm2_ctx *ctx, int nsplit, double dt, const double *AbsTol, const double *RelTol,
+                    double *RPAR, int *IPAR, int use_graph);
+
+/* Per-cell outcome of the last integration (any pointer may be NULL):
+ * status (1 ok, -6 step cap, -7 step too small, -8 singular), accepted and
+ * rejected step counts, first accepted step size and exit step size. */
+int radm2_get_cell_stats(radm2_ctx *ctx, int *status, int *nacc, int *nrej, double *hfirst, double *hexit);
+int radm2_get_stats(radm2_ctx *ctx, radm2_stats *out);
+
+/* Per-cell starting step override (device order = cell order), NULL clears it.
+ * Values outside (0, Hmax] or non-finite fall back to the default Hstart. */
+int radm2_set_cell_hstart(radm2_ctx *ctx, const double *h0);
+/* Cell visiting order for the persistent schedule (a permutation of 0..ncell-1),
+ * NULL restores natural order. */
+int radm2_set_cell_order(radm2_ctx *ctx, const int *order);
+
+/*
+ * Batched mechanism kernels on caller arrays (host pointers, per-cell layout), the
+ * counterparts of the reference's Fun(), Jac(), Decomp() and Solve() host wrappers
+ * (mgpu.cu:1391-1424, 2654-2683, 2849-2852, 3123-3126):
+ *   radm2_fun          VDOT[n][59] = F(V)        with FIX[n][2], RCT[n][156]
+ *   radm2_jac          JVS[n][659] = J(V)        in LU slot order
+ *   radm2_decomp_solve G[n][659] factored in place (pivot-free, fixed pattern) and
+ *                      X[n][59] overwritten with G^-1 X; sing[n] = zero-pivot row + 1
+ *                      or 0.  precision RADM2_PREC_FP32LU factors in float.
+ * They allocate temporary device buffers per call (not for hot loops).
+ */
+int radm2_fun(radm2_ctx *ctx, int n, const double *V, const double *FIX, const double *RCT, double *VDOT);
+int radm2_jac(radm2_ctx *ctx, int n, const double *V, const double *FIX, const double *RCT, double *JVS);
+int radm2_decomp_solve(radm2_ctx *ctx, int n, int precision, double *G, double *X, int *sing);
+
+/* Solver-kernel timing: when enabled, CUDA events bracket every solver-kernel launch
+ * on the context's stream (graph replays included).  radm2_get_kernel_time returns
+ * the summed device time (ms) and launch count since the previous call. */
+int radm2_set_kernel_timing(radm2_ctx *ctx, int enable);
+int radm2_get_kernel_time(radm2_ctx *ctx, double *ms, int *launches);
+
+/* Measured CUDA-core FMA throughput of a device (TFLOP/s, 2 flops per FMA): the
+ * denominators of the solver's roofline.  Runs ~0.2 s of microbenchmark. */
+int radm2_fma_peak(int device, double *fp64_tflops, double *fp32_tflops);
+
+/* Number of cells and device bytes held by the context. */
+int radm2_get_ncell(const radm2_ctx *ctx);
+size_t radm2_device_bytes(const radm2_ctx *ctx);
+
+/* Host-only consistency check of the library's kernel layouts (every thread's
+ * working-set offsets inside its allocation, for every built variant). */
+int radm2_selfcheck(void);
+
+/* Library build string (arch, variants). */
+const char *radm2_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

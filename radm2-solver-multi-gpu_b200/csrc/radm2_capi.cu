@@ -1,0 +1,882 @@
+// C ABI of the B200 RADM2 solver (include/radm2.h): context, device buffers,
+// IPAR/RPAR parsing with the reference's checks, kernel launches and the
+// CUDA-graph operator-split loop.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/radm2.h"
+#include "radm2_internal.h"
+
+using namespace radm2;
+
+struct radm2_ctx {
+    radm2_opts o{};
+    int nsm = 0;
+    cudaStream_t own = nullptr;
+    cudaStream_t st = nullptr;
+    int ncell = 0, ld = 0;
+    double *var = nullptr, *fix = nullptr, *temp = nullptr, *rcn = nullptr, *jv = nullptr, *rconst = nullptr;
+    bool have_rcn = false;
+    bool rconst_valid = false;
+    double *h0 = nullptr;
+    int *order = nullptr;
+    int *status = nullptr, *nacc = nullptr, *nrej = nullptr;
+    double *hfirst = nullptr, *hexit = nullptr, *texit = nullptr;
+    int *queue = nullptr;  // one counter per split
+    int queue_cap = 0;
+    double *scratch = nullptr;
+    size_t scratch_bytes = 0;
+    double *stage = nullptr;
+    size_t stage_bytes = 0;
+    void *partials = nullptr;
+    RunResult *d_res = nullptr, *h_res = nullptr;
+    int res_cap = 0;
+    size_t bytes = 0;
+    std::string err;
+    radm2_stats stats{};
+    // cached split graph
+    cudaGraphExec_t gexec = nullptr;
+    std::vector<unsigned char> gkey;
+    // solver-kernel timing
+    bool timing = false;
+    std::vector<cudaEvent_t> ev;  // start/stop pairs, one per result slot
+    int ev_used = 0;
+    double kernel_ms = 0.0;
+    int kernel_launches = 0;
+};
+
+namespace {
+
+int fail_cuda(radm2_ctx *c, cudaError_t e, const char *what)
+{
+    c->err = std::string(what) + ": " + cudaGetErrorString(e);
+    if (e == cudaErrorMemoryAllocation) return RADM2_E_NOMEM;
+    return RADM2_E_CUDA;
+}
+
+#define CK(call)                                          \
+    do {                                                  \
+        cudaError_t e_ = (call);                          \
+        if (e_ != cudaSuccess) return fail_cuda(c, e_, #call); \
+    } while (0)
+
+template <typename T>
+int dalloc(radm2_ctx *c, T **p, size_t count)
+{
+    if (*p) {
+        cudaFree(*p);
+        *p = nullptr;
+    }
+    if (count == 0) return RADM2_OK;
+    cudaError_t e = cudaMalloc((void **)p, count * sizeof(T));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return fail_cuda(c, e, "cudaMalloc");
+    }
+    c->bytes += count * sizeof(T);
+    return RADM2_OK;
+}
+
+void free_cells(radm2_ctx *c)
+{
+    void *ptrs[] = {c->var, c->fix, c->temp, c->rcn, c->jv, c->rconst, c->h0, c->order, c->status,
+                    c->nacc, c->nrej, c->hfirst, c->hexit, c->texit};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    c->var = c->fix = c->temp = c->rcn = c->jv = c->rconst = nullptr;
+    c->h0 = nullptr;
+    c->order = nullptr;
+    c->status = c->nacc = c->nrej = nullptr;
+    c->hfirst = c->hexit = c->texit = nullptr;
+    c->ncell = c->ld = 0;
+    c->rconst_valid = false;
+}
+
+void drop_graph(radm2_ctx *c)
+{
+    if (c->gexec) cudaGraphExecDestroy(c->gexec);
+    c->gexec = nullptr;
+    c->gkey.clear();
+}
+
+int ensure_cells(radm2_ctx *c, int ncell)
+{
+    if (ncell == c->ncell && c->var) return RADM2_OK;
+    drop_graph(c);
+    free_cells(c);
+    const int ld = (ncell + 31) / 32 * 32;
+    int rc;
+    if ((rc = dalloc(c, &c->var, (size_t)NVAR * ld))) return rc;
+    if ((rc = dalloc(c, &c->fix, (size_t)NFIX * ld))) return rc;
+    if ((rc = dalloc(c, &c->temp, (size_t)ld))) return rc;
+    if ((rc = dalloc(c, &c->rcn, (size_t)ld))) return rc;
+    if ((rc = dalloc(c, &c->jv, (size_t)NPH * ld))) return rc;
+    if ((rc = dalloc(c, &c->rconst, (size_t)NREACT * ld))) return rc;
+    if ((rc = dalloc(c, &c->status, (size_t)ld))) return rc;
+    if ((rc = dalloc(c, &c->nacc, (size_t)ld))) return rc;
+    if ((rc = dalloc(c, &c->nrej, (size_t)ld))) return rc;
+    if ((rc = dalloc(c, &c->hfirst, (size_t)ld))) return rc;
+    if ((rc = dalloc(c, &c->hexit, (size_t)ld))) return rc;
+    if ((rc = dalloc(c, &c->texit, (size_t)ld))) return rc;
+    c->ncell = ncell;
+    c->ld = ld;
+    return RADM2_OK;
+}
+
+int ensure_stage(radm2_ctx *c, size_t bytes)
+{
+    if (bytes <= c->stage_bytes) return RADM2_OK;
+    if (c->stage) cudaFree(c->stage);
+    c->stage = nullptr;
+    c->stage_bytes = 0;
+    CK(cudaMalloc((void **)&c->stage, bytes));
+    c->stage_bytes = bytes;
+    return RADM2_OK;
+}
+
+int ensure_results(radm2_ctx *c, int n)
+{
+    if (n <= c->res_cap) return RADM2_OK;
+    drop_graph(c);
+    if (c->d_res) cudaFree(c->d_res);
+    if (c->h_res) cudaFreeHost(c->h_res);
+    if (c->queue) cudaFree(c->queue);
+    c->d_res = nullptr;
+    c->h_res = nullptr;
+    c->queue = nullptr;
+    c->res_cap = 0;
+    CK(cudaMalloc((void **)&c->d_res, sizeof(RunResult) * n));
+    CK(cudaMallocHost((void **)&c->h_res, sizeof(RunResult) * n));
+    CK(cudaMalloc((void **)&c->queue, sizeof(int) * n));
+    c->res_cap = n;
+    return RADM2_OK;
+}
+
+// Upload host AoS [n][m] into device SoA [m][ld] through the staging buffer.
+int upload_aos(radm2_ctx *c, const double *host, int m, double *dst)
+{
+    const size_t bytes = (size_t)c->ncell * m * sizeof(double);
+    int rc = ensure_stage(c, bytes);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(c->stage, host, bytes, cudaMemcpyHostToDevice, c->st));
+    CK(launch_aos_to_soa(c->ncell, m, c->ld, c->stage, dst, c->st));
+    return RADM2_OK;
+}
+
+int download_aos(radm2_ctx *c, const double *src, int m, double *host)
+{
+    const size_t bytes = (size_t)c->ncell * m * sizeof(double);
+    int rc = ensure_stage(c, bytes);
+    if (rc) return rc;
+    CK(launch_soa_to_aos(c->ncell, m, c->ld, src, c->stage, c->st));
+    CK(cudaMemcpyAsync(host, c->stage, bytes, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return RADM2_OK;
+}
+
+// Unit roundoff computed as mgpu.cu:949-973 does (halving until 1 + eps == 1).
+double wlamch()
+{
+    double eps = std::pow(0.5, 16);
+    int i;
+    for (i = 17; i <= 80; i++) {
+        eps = eps * 0.5;
+        volatile double suma = 1.0 + eps;
+        if (suma <= 1.0) break;
+    }
+    if (i == 80) return 2.2e-16;
+    return eps * 2.0;
+}
+
+inline double maxh(double a, double b) { return (a >= b) ? a : b; }
+inline double minh(double b, double c) { return (b < c) ? b : c; }
+inline double absh(double x) { return (x >= 0) ? x : -x; }
+
+// IPAR/RPAR parsing and validation, mgpu.cu:3684-3811 (same checks, same order, same codes).
+int parse_params(double Tstart, double Tend, const double *AbsTol, const double *RelTol, const double *RPAR,
+                 const int *IPAR, int float_coeffs, SolveParams *p, int *autonomous)
+{
+    static const double ros_M[3] = {RADM2_ROS_M0, RADM2_ROS_M1, RADM2_ROS_M2};
+    static const double ros_E[3] = {RADM2_ROS_E0, RADM2_ROS_E1, RADM2_ROS_E2};
+    std::memset(p, 0, sizeof *p);
+    p->Tstart = Tstart;
+    p->Tend = Tend;
+    *autonomous = !(IPAR[0] == 0);
+    const bool vector_tol = (IPAR[1] == 0);
+    const int uplim = vector_tol ? NVAR : 1;
+    int max_steps = (IPAR[2] == 0) ? 100000 : IPAR[2];
+    if (max_steps < 0) return -1;
+    if ((IPAR[3] < 1) || (IPAR[3] > 5)) return -2;
+    p->Roundoff = wlamch();
+    p->Hmin = RPAR[0];
+    if (RPAR[0] < 0.0) return -3;
+    p->Hmax = (RPAR[1] == 0.0) ? absh(Tend - Tstart) : minh(absh(RPAR[1]), absh(Tend - Tstart));
+    if (RPAR[1] < 0.0) return -3;
+    p->Hstart = (RPAR[2] == 0.0) ? maxh(p->Hmin, DELTA_MIN) : minh(absh(RPAR[2]), absh(Tend - Tstart));
+    if (RPAR[2] < 0.0) return -3;
+    p->FacMin = (RPAR[3] == 0.0) ? 0.2 : RPAR[3];
+    if (RPAR[3] < 0.0) return -4;
+    p->FacMax = (RPAR[4] == 0.0) ? 6.0 : RPAR[4];
+    if (RPAR[4] < 0.0) return -4;
+    p->FacRej = (RPAR[5] == 0.0) ? 0.1 : RPAR[5];
+    if (RPAR[5] < 0.0) return -4;
+    p->FacSafe = (RPAR[6] == 0.0) ? 0.9 : RPAR[6];
+    if (RPAR[6] < 0.0) return -4;
+    for (int i = 0; i < uplim; i++)
+        if ((AbsTol[i] <= 0.0) || (RelTol[i] <= 10.0 * p->Roundoff) || (RelTol[i] >= 1.0)) return -5;
+    if (IPAR[3] != 2) return -2;  // only ROS-3 is wired (mgpu.cu:3803-3811)
+    for (int i = 0; i < NVAR; i++) {
+        p->AbsTol[i] = vector_tol ? AbsTol[i] : AbsTol[0];
+        p->RelTol[i] = vector_tol ? RelTol[i] : RelTol[0];
+    }
+    for (int i = 0; i < 3; i++) {
+        p->M[i] = float_coeffs ? (double)(float)ros_M[i] : ros_M[i];
+        p->E[i] = float_coeffs ? (double)(float)ros_E[i] : ros_E[i];
+    }
+    p->max_steps = max_steps;
+    p->direction = (Tend >= Tstart) ? +1 : -1;
+    return 1;
+}
+
+int key_of(const radm2_ctx *c, int bs)
+{
+    return variant_key(bs, c->o.placement, c->o.min_blocks > 1 ? c->o.min_blocks : 1);
+}
+
+cudaError_t variant_info(radm2_ctx *c, int bs, SolverInfo *info)
+{
+    const bool fp32 = c->o.precision == RADM2_PREC_FP32LU;
+    const bool pers = c->o.schedule == RADM2_SCHED_PERSISTENT;
+    const int k = key_of(c, bs);
+    if (fp32) return pers ? solver_info_fp32_persistent(k, info) : solver_info_fp32_static(k, info);
+    return pers ? solver_info_fp64_persistent(k, info) : solver_info_fp64_static(k, info);
+}
+
+int default_block_threads(const radm2_opts &o)
+{
+    if (o.placement == RADM2_PLACE_GLOBAL) return 128;
+    if (o.placement == RADM2_PLACE_LU_SMEM && o.precision == RADM2_PREC_FP32LU) return 64;
+    return 32;
+}
+
+int launch_geometry(radm2_ctx *c, int *bs_out, int *grid_out, size_t *scratch_out)
+{
+    const int bs = c->o.block_threads ? c->o.block_threads : default_block_threads(c->o);
+    SolverInfo info;
+    cudaError_t e = variant_info(c, bs, &info);
+    if (e != cudaSuccess || info.blocks_per_sm < 1) {
+        c->err = "solver variant not built for this precision/placement/block size";
+        (void)cudaGetLastError();
+        return RADM2_E_ARG;
+    }
+    int grid;
+    if (c->o.schedule == RADM2_SCHED_PERSISTENT) {
+        int bpsm = c->o.blocks_per_sm > 0 ? c->o.blocks_per_sm : info.blocks_per_sm;
+        if (bpsm > info.blocks_per_sm) bpsm = info.blocks_per_sm;
+        grid = c->nsm * bpsm;
+        const int need = (c->ncell + bs - 1) / bs;
+        if (grid > need) grid = need;
+    } else {
+        grid = (c->ncell + bs - 1) / bs;
+    }
+    if (grid < 1) grid = 1;
+    *bs_out = bs;
+    *grid_out = grid;
+    *scratch_out = (size_t)grid * bs * info.global_words * sizeof(double);
+    return RADM2_OK;
+}
+
+int ensure_scratch(radm2_ctx *c, size_t bytes)
+{
+    if (bytes <= c->scratch_bytes) return RADM2_OK;
+    drop_graph(c);
+    if (c->scratch) cudaFree(c->scratch);
+    c->scratch = nullptr;
+    c->scratch_bytes = 0;
+    CK(cudaMalloc((void **)&c->scratch, bytes));
+    c->scratch_bytes = bytes;
+    return RADM2_OK;
+}
+
+SolveArgs make_args(radm2_ctx *c, const SolveParams &p, int *queue)
+{
+    SolveArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.p = p;
+    a.ncell = c->ncell;
+    a.ld = c->ld;
+    a.var = c->var;
+    a.fix = c->fix;
+    a.rconst = c->rconst;
+    a.h0 = c->h0;
+    a.order = c->order;
+    a.queue = queue;
+    a.scratch = c->scratch;
+    a.status = c->status;
+    a.nacc = c->nacc;
+    a.nrej = c->nrej;
+    a.hfirst = c->hfirst;
+    a.hexit = c->hexit;
+    a.texit = c->texit;
+    a.refine = c->o.refine_sweeps;
+    return a;
+}
+
+cudaError_t launch_solver(radm2_ctx *c, const SolveArgs &a, int bs, int grid)
+{
+    const bool fp32 = c->o.precision == RADM2_PREC_FP32LU;
+    const bool pers = c->o.schedule == RADM2_SCHED_PERSISTENT;
+    const int k = key_of(c, bs);
+    if (fp32)
+        return pers ? launch_solver_fp32_persistent(a, k, grid, c->st) : launch_solver_fp32_static(a, k, grid, c->st);
+    return pers ? launch_solver_fp64_persistent(a, k, grid, c->st) : launch_solver_fp64_static(a, k, grid, c->st);
+}
+
+// Enqueue one integration of every cell: queue reset, solver, outcome reduction into d_res[slot].
+int enqueue_integration(radm2_ctx *c, const SolveParams &p, int slot, int bs, int grid)
+{
+    CK(cudaMemsetAsync(c->queue + slot, 0, sizeof(int), c->st));
+    SolveArgs a = make_args(c, p, c->queue + slot);
+    if (c->timing) {
+        while ((int)c->ev.size() < 2 * (slot + 1)) {
+            cudaEvent_t e;
+            CK(cudaEventCreate(&e));
+            c->ev.push_back(e);
+        }
+        CK(cudaEventRecord(c->ev[2 * slot], c->st));
+    }
+    CK(launch_solver(c, a, bs, grid));
+    if (c->timing) {
+        CK(cudaEventRecord(c->ev[2 * slot + 1], c->st));
+        if (slot + 1 > c->ev_used) c->ev_used = slot + 1;
+    }
+    CK(launch_reduce(c->ncell, c->status, c->nacc, c->nrej, c->texit, c->hexit, c->partials, c->d_res + slot, c->st));
+    return RADM2_OK;
+}
+
+int ensure_rconst(radm2_ctx *c)
+{
+    if (c->rconst_valid) return RADM2_OK;
+    CK(launch_rconst(c->ncell, c->ld, c->jv, c->temp, c->fix, c->have_rcn ? c->rcn : nullptr, c->rconst, c->st));
+    c->rconst_valid = true;
+    return RADM2_OK;
+}
+
+// Fold results of nres integrations into IPAR/RPAR/stats; returns IERR.
+int finish(radm2_ctx *c, int nres, int autonomous, double *RPAR, int *IPAR, int direction)
+{
+    if (c->timing) {
+        for (int i = 0; i < c->ev_used && i < nres; i++) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, c->ev[2 * i], c->ev[2 * i + 1]) == cudaSuccess) {
+                c->kernel_ms += ms;
+                c->kernel_launches++;
+            } else {
+                (void)cudaGetLastError();
+            }
+        }
+        c->ev_used = 0;
+    }
+    long long nacc = 0, nrej = 0, nfail = 0;
+    int worst = 1, max_att = 0;
+    double tmin = 0, tmax = 0, hmin = 0;
+    for (int i = 0; i < nres; i++) {
+        const RunResult &r = c->h_res[i];
+        nacc += r.nacc;
+        nrej += r.nrej;
+        nfail += r.nfail;
+        if (r.worst < worst) worst = r.worst;
+        if (r.max_att > max_att) max_att = r.max_att;
+        if (i == nres - 1) {
+            tmin = r.tmin;
+            tmax = r.tmax;
+            hmin = r.hmin;
+        }
+    }
+    const long long natt = nacc + nrej;
+    const long long nouter = nacc + nfail;
+    IPAR[10] += (int)(nouter * (autonomous ? 1 : 2) + natt);  // Nfun
+    IPAR[11] += (int)nouter;                                   // Njac
+    IPAR[12] += (int)natt;                                     // Nstp
+    IPAR[13] += (int)nacc;                                     // Nacc
+    IPAR[14] += (int)nrej;                                     // Nrej
+    IPAR[15] += (int)natt;                                     // Ndec
+    IPAR[16] += (int)(3 * natt);                               // Nsol
+    RPAR[10] = direction > 0 ? tmin : tmax;
+    RPAR[11] = hmin;
+    c->stats.n_accepted = nacc;
+    c->stats.n_rejected = nrej;
+    c->stats.n_failed = nfail;
+    c->stats.worst_status = worst;
+    c->stats.max_steps_cell = max_att;
+    c->stats.texit_min = RPAR[10];
+    c->stats.hexit_min = hmin;
+    return worst;
+}
+
+bool valid_ctx(const radm2_ctx *c) { return c != nullptr; }
+
+}  // namespace
+
+extern "C" {
+
+int radm2_opts_default(radm2_opts *o)
+{
+    if (!o) return RADM2_E_ARG;
+    std::memset(o, 0, sizeof *o);
+    o->device = 0;
+    o->precision = RADM2_PREC_FP64;
+    o->refine_sweeps = 1;
+    o->schedule = RADM2_SCHED_STATIC;
+    o->block_threads = 0;
+    o->blocks_per_sm = 0;
+    o->float_coeffs = 1;
+    o->placement = RADM2_PLACE_GLOBAL;
+    o->min_blocks = 0;
+    return RADM2_OK;
+}
+
+int radm2_create(radm2_ctx **out, const radm2_opts *opts)
+{
+    if (!out) return RADM2_E_ARG;
+    *out = nullptr;
+    radm2_opts o;
+    if (opts)
+        o = *opts;
+    else
+        radm2_opts_default(&o);
+    if (o.precision != RADM2_PREC_FP64 && o.precision != RADM2_PREC_FP32LU) return RADM2_E_ARG;
+    if (o.schedule != RADM2_SCHED_STATIC && o.schedule != RADM2_SCHED_PERSISTENT) return RADM2_E_ARG;
+    if (o.refine_sweeps < 0 || o.refine_sweeps > 2) return RADM2_E_ARG;
+    if (o.placement != RADM2_PLACE_GLOBAL && o.placement != RADM2_PLACE_LU_SMEM && o.placement != RADM2_PLACE_ALL_SMEM)
+        return RADM2_E_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= o.device || o.device < 0) return RADM2_E_NODEV;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, o.device) != cudaSuccess) return RADM2_E_NODEV;
+    if (prop.major != 10) return RADM2_E_NODEV;  // built for sm_100a only
+    radm2_ctx *c = new radm2_ctx();
+    c->o = o;
+    c->nsm = prop.multiProcessorCount;
+    if (cudaSetDevice(o.device) != cudaSuccess || cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return RADM2_E_CUDA;
+    }
+    c->st = c->own;
+    if (cudaMalloc(&c->partials, reduce_partials_bytes()) != cudaSuccess || ensure_results(c, 8) != RADM2_OK) {
+        radm2_destroy(c);
+        return RADM2_E_NOMEM;
+    }
+    *out = c;
+    return RADM2_OK;
+}
+
+int radm2_destroy(radm2_ctx *c)
+{
+    if (!c) return RADM2_E_ARG;
+    cudaSetDevice(c->o.device);
+    if (c->st) cudaStreamSynchronize(c->st);
+    drop_graph(c);
+    free_cells(c);
+    for (cudaEvent_t e : c->ev) cudaEventDestroy(e);
+    if (c->scratch) cudaFree(c->scratch);
+    if (c->stage) cudaFree(c->stage);
+    if (c->partials) cudaFree(c->partials);
+    if (c->d_res) cudaFree(c->d_res);
+    if (c->h_res) cudaFreeHost(c->h_res);
+    if (c->queue) cudaFree(c->queue);
+    if (c->own) cudaStreamDestroy(c->own);
+    delete c;
+    return RADM2_OK;
+}
+
+const char *radm2_error_string(int code)
+{
+    switch (code) {
+        case 1: return "success";
+        case 0: return "ok";
+        case -1: return "Improper value for maximal no of steps";
+        case -2: return "Selected Rosenbrock method not implemented";
+        case -3: return "Hmin/Hmax/Hstart must be positive";
+        case -4: return "FacMin/FacMax/FacRej must be positive";
+        case -5: return "Improper tolerance values";
+        case -6: return "No of steps exceeds maximum bound";
+        case -7: return "Step size too small (T + H/10 = T) or H < Roundoff";
+        case -8: return "Matrix is repeatedly singular";
+        case RADM2_E_ARG: return "invalid argument";
+        case RADM2_E_CUDA: return "CUDA runtime error";
+        case RADM2_E_NOMEM: return "device allocation failed";
+        case RADM2_E_STATE: return "call out of order";
+        case RADM2_E_NODEV: return "no usable sm_100 device";
+        case RADM2_E_TOOBIG: return "size exceeds the documented maximum";
+        default: return "unknown error code";
+    }
+}
+
+const char *radm2_last_error(const radm2_ctx *c) { return c ? c->err.c_str() : "null context"; }
+
+int radm2_set_stream(radm2_ctx *c, void *stream)
+{
+    if (!valid_ctx(c)) return RADM2_E_ARG;
+    drop_graph(c);
+    c->st = stream ? (cudaStream_t)stream : c->own;
+    return RADM2_OK;
+}
+
+int radm2_synchronize(radm2_ctx *c)
+{
+    if (!valid_ctx(c)) return RADM2_E_ARG;
+    CK(cudaStreamSynchronize(c->st));
+    return RADM2_OK;
+}
+
+int radm2_set_inputs(radm2_ctx *c, int ncell, const double *VAR, const double *FIX, const double *TEMP,
+                     const double *RC_N2O5, const double *JV)
+{
+    if (!valid_ctx(c) || ncell <= 0 || !VAR || !FIX || !TEMP || !JV) return RADM2_E_ARG;
+    CK(cudaSetDevice(c->o.device));
+    int rc = ensure_cells(c, ncell);
+    if (rc) return rc;
+    if ((rc = upload_aos(c, VAR, NVAR, c->var))) return rc;
+    if ((rc = upload_aos(c, FIX, NFIX, c->fix))) return rc;
+    if ((rc = upload_aos(c, JV, NPH, c->jv))) return rc;
+    CK(cudaMemcpyAsync(c->temp, TEMP, sizeof(double) * ncell, cudaMemcpyHostToDevice, c->st));
+    c->have_rcn = RC_N2O5 != nullptr;
+    if (RC_N2O5) CK(cudaMemcpyAsync(c->rcn, RC_N2O5, sizeof(double) * ncell, cudaMemcpyHostToDevice, c->st));
+    c->rconst_valid = false;
+    return RADM2_OK;
+}
+
+int radm2_set_state(radm2_ctx *c, const double *VAR)
+{
+    if (!valid_ctx(c) || !VAR) return RADM2_E_ARG;
+    if (!c->var) return RADM2_E_STATE;
+    return upload_aos(c, VAR, NVAR, c->var);
+}
+
+int radm2_get_state(radm2_ctx *c, double *VAR)
+{
+    if (!valid_ctx(c) || !VAR) return RADM2_E_ARG;
+    if (!c->var) return RADM2_E_STATE;
+    return download_aos(c, c->var, NVAR, VAR);
+}
+
+int radm2_set_inputs_device(radm2_ctx *c, int ncell, int ld, const double *var, const double *fix,
+                            const double *temp, const double *rc_n2o5, const double *jv)
+{
+    if (!valid_ctx(c) || ncell <= 0 || ld < ncell || !var || !fix || !temp || !jv) return RADM2_E_ARG;
+    CK(cudaSetDevice(c->o.device));
+    int rc = ensure_cells(c, ncell);
+    if (rc) return rc;
+    const size_t w = sizeof(double) * ncell, sp = sizeof(double) * ld, dp = sizeof(double) * c->ld;
+    CK(cudaMemcpy2DAsync(c->var, dp, var, sp, w, NVAR, cudaMemcpyDeviceToDevice, c->st));
+    CK(cudaMemcpy2DAsync(c->fix, dp, fix, sp, w, NFIX, cudaMemcpyDeviceToDevice, c->st));
+    CK(cudaMemcpy2DAsync(c->jv, dp, jv, sp, w, NPH, cudaMemcpyDeviceToDevice, c->st));
+    CK(cudaMemcpyAsync(c->temp, temp, w, cudaMemcpyDeviceToDevice, c->st));
+    c->have_rcn = rc_n2o5 != nullptr;
+    if (rc_n2o5) CK(cudaMemcpyAsync(c->rcn, rc_n2o5, w, cudaMemcpyDeviceToDevice, c->st));
+    c->rconst_valid = false;
+    return RADM2_OK;
+}
+
+int radm2_get_state_device(radm2_ctx *c, double *var, int ld)
+{
+    if (!valid_ctx(c) || !var || ld < c->ncell) return RADM2_E_ARG;
+    if (!c->var) return RADM2_E_STATE;
+    CK(cudaMemcpy2DAsync(var, sizeof(double) * ld, c->var, sizeof(double) * c->ld, sizeof(double) * c->ncell, NVAR,
+                         cudaMemcpyDeviceToDevice, c->st));
+    return RADM2_OK;
+}
+
+int radm2_set_state_device(radm2_ctx *c, const double *var, int ld)
+{
+    if (!valid_ctx(c) || !var || ld < c->ncell) return RADM2_E_ARG;
+    if (!c->var) return RADM2_E_STATE;
+    CK(cudaMemcpy2DAsync(c->var, sizeof(double) * c->ld, var, sizeof(double) * ld, sizeof(double) * c->ncell, NVAR,
+                         cudaMemcpyDeviceToDevice, c->st));
+    return RADM2_OK;
+}
+
+int radm2_update_rconst(radm2_ctx *c)
+{
+    if (!valid_ctx(c)) return RADM2_E_ARG;
+    if (!c->var) return RADM2_E_STATE;
+    c->rconst_valid = false;
+    return ensure_rconst(c);
+}
+
+int radm2_get_rconst(radm2_ctx *c, double *RCONST)
+{
+    if (!valid_ctx(c) || !RCONST) return RADM2_E_ARG;
+    if (!c->var) return RADM2_E_STATE;
+    int rc = ensure_rconst(c);
+    if (rc) return rc;
+    return download_aos(c, c->rconst, NREACT, RCONST);
+}
+
+int radm2_set_rconst(radm2_ctx *c, const double *RCONST)
+{
+    if (!valid_ctx(c) || !RCONST) return RADM2_E_ARG;
+    if (!c->var) return RADM2_E_STATE;
+    int rc = upload_aos(c, RCONST, NREACT, c->rconst);
+    if (rc) return rc;
+    c->rconst_valid = true;
+    return RADM2_OK;
+}
+
+int radm2_rosenbrock(radm2_ctx *c, double Tstart, double Tend, const double *AbsTol, const double *RelTol,
+                     double *RPAR, int *IPAR)
+{
+    if (!valid_ctx(c) || !AbsTol || !RelTol || !RPAR || !IPAR) return RADM2_E_ARG;
+    if (!c->var) return RADM2_E_STATE;
+    CK(cudaSetDevice(c->o.device));
+    SolveParams p;
+    int autonomous = 1;
+    int ierr = parse_params(Tstart, Tend, AbsTol, RelTol, RPAR, IPAR, c->o.float_coeffs, &p, &autonomous);
+    if (ierr != 1) return ierr;
+    int rc = ensure_rconst(c);
+    if (rc) return rc;
+    int bs, grid;
+    size_t sbytes;
+    if ((rc = launch_geometry(c, &bs, &grid, &sbytes))) return rc;
+    if ((rc = ensure_scratch(c, sbytes))) return rc;
+    if ((rc = enqueue_integration(c, p, 0, bs, grid))) return rc;
+    CK(cudaMemcpyAsync(c->h_res, c->d_res, sizeof(RunResult), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return finish(c, 1, autonomous, RPAR, IPAR, p.direction);
+}
+
+int radm2_run_split(radm2_ctx *c, int nsplit, double dt, const double *AbsTol, const double *RelTol, double *RPAR,
+                    int *IPAR, int use_graph)
+{
+    if (!valid_ctx(c) || nsplit <= 0 || !(dt > 0.0) || !AbsTol || !RelTol || !RPAR || !IPAR) return RADM2_E_ARG;
+    if (!c->var) return RADM2_E_STATE;
+    CK(cudaSetDevice(c->o.device));
+    double rpar[20];
+    std::memcpy(rpar, RPAR, sizeof rpar);
+    if (rpar[2] == 0.0) rpar[2] = 0.01 * dt;  // the reference driver's Hstart ratio (mgpu.cu:3873)
+    SolveParams p;
+    int autonomous = 1;
+    int ierr = parse_params(0.0, dt, AbsTol, RelTol, rpar, IPAR, c->o.float_coeffs, &p, &autonomous);
+    if (ierr != 1) return ierr;
+    int rc = ensure_rconst(c);
+    if (rc) return rc;
+    int bs, grid;
+    size_t sbytes;
+    if ((rc = launch_geometry(c, &bs, &grid, &sbytes))) return rc;
+    if ((rc = ensure_scratch(c, sbytes))) return rc;
+    if ((rc = ensure_results(c, nsplit))) return rc;
+    if (!use_graph) {
+        for (int s = 0; s < nsplit; s++)
+            if ((rc = enqueue_integration(c, p, s, bs, grid))) return rc;
+        CK(cudaMemcpyAsync(c->h_res, c->d_res, sizeof(RunResult) * nsplit, cudaMemcpyDeviceToHost, c->st));
+    } else {
+        // The graph bakes in the launch arguments; rebuild it when any of them change.
+        std::vector<unsigned char> key(sizeof(SolveArgs) + 4 * sizeof(int));
+        SolveArgs a0 = make_args(c, p, c->queue);
+        std::memcpy(key.data(), &a0, sizeof a0);
+        int extra[4] = {nsplit, bs, grid, (int)(c->o.precision * 4096 + c->o.schedule * 2048 + key_of(c, bs))};
+        std::memcpy(key.data() + sizeof a0, extra, sizeof extra);
+        if (!c->gexec || key != c->gkey) {
+            drop_graph(c);
+            cudaGraph_t g;
+            CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+            for (int s = 0; s < nsplit && rc == RADM2_OK; s++) rc = enqueue_integration(c, p, s, bs, grid);
+            if (rc == RADM2_OK) {
+                cudaError_t e = cudaMemcpyAsync(c->h_res, c->d_res, sizeof(RunResult) * nsplit,
+                                                cudaMemcpyDeviceToHost, c->st);
+                if (e != cudaSuccess) rc = fail_cuda(c, e, "capture memcpy");
+            }
+            cudaError_t e = cudaStreamEndCapture(c->st, &g);
+            if (rc) return rc;
+            if (e != cudaSuccess) return fail_cuda(c, e, "cudaStreamEndCapture");
+            e = cudaGraphInstantiate(&c->gexec, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) {
+                c->gexec = nullptr;
+                return fail_cuda(c, e, "cudaGraphInstantiate");
+            }
+            c->gkey = key;
+        }
+        if (c->timing) c->ev_used = nsplit;  // the graph's event nodes re-record every replay
+        CK(cudaGraphLaunch(c->gexec, c->st));
+    }
+    CK(cudaStreamSynchronize(c->st));
+    return finish(c, nsplit, autonomous, RPAR, IPAR, p.direction);
+}
+
+int radm2_get_cell_stats(radm2_ctx *c, int *status, int *nacc, int *nrej, double *hfirst, double *hexit)
+{
+    if (!valid_ctx(c)) return RADM2_E_ARG;
+    if (!c->var) return RADM2_E_STATE;
+    const int n = c->ncell;
+    if (status) CK(cudaMemcpyAsync(status, c->status, sizeof(int) * n, cudaMemcpyDeviceToHost, c->st));
+    if (nacc) CK(cudaMemcpyAsync(nacc, c->nacc, sizeof(int) * n, cudaMemcpyDeviceToHost, c->st));
+    if (nrej) CK(cudaMemcpyAsync(nrej, c->nrej, sizeof(int) * n, cudaMemcpyDeviceToHost, c->st));
+    if (hfirst) CK(cudaMemcpyAsync(hfirst, c->hfirst, sizeof(double) * n, cudaMemcpyDeviceToHost, c->st));
+    if (hexit) CK(cudaMemcpyAsync(hexit, c->hexit, sizeof(double) * n, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return RADM2_OK;
+}
+
+int radm2_get_stats(radm2_ctx *c, radm2_stats *out)
+{
+    if (!valid_ctx(c) || !out) return RADM2_E_ARG;
+    *out = c->stats;
+    return RADM2_OK;
+}
+
+int radm2_set_cell_hstart(radm2_ctx *c, const double *h0)
+{
+    if (!valid_ctx(c)) return RADM2_E_ARG;
+    if (!c->var) return RADM2_E_STATE;
+    drop_graph(c);
+    if (!h0) {
+        if (c->h0) cudaFree(c->h0);
+        c->h0 = nullptr;
+        return RADM2_OK;
+    }
+    if (!c->h0) CK(cudaMalloc((void **)&c->h0, sizeof(double) * c->ld));
+    CK(cudaMemcpyAsync(c->h0, h0, sizeof(double) * c->ncell, cudaMemcpyHostToDevice, c->st));
+    return RADM2_OK;
+}
+
+int radm2_set_cell_order(radm2_ctx *c, const int *order)
+{
+    if (!valid_ctx(c)) return RADM2_E_ARG;
+    if (!c->var) return RADM2_E_STATE;
+    drop_graph(c);
+    if (!order) {
+        if (c->order) cudaFree(c->order);
+        c->order = nullptr;
+        return RADM2_OK;
+    }
+    std::vector<char> seen(c->ncell, 0);
+    for (int i = 0; i < c->ncell; i++) {
+        if (order[i] < 0 || order[i] >= c->ncell || seen[order[i]]) {
+            c->err = "cell order is not a permutation";
+            return RADM2_E_ARG;
+        }
+        seen[order[i]] = 1;
+    }
+    if (!c->order) CK(cudaMalloc((void **)&c->order, sizeof(int) * c->ld));
+    CK(cudaMemcpyAsync(c->order, order, sizeof(int) * c->ncell, cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return RADM2_OK;
+}
+
+int radm2_set_kernel_timing(radm2_ctx *c, int enable)
+{
+    if (!valid_ctx(c)) return RADM2_E_ARG;
+    drop_graph(c);  // captured graphs must be rebuilt with (or without) the event nodes
+    c->timing = enable != 0;
+    c->kernel_ms = 0.0;
+    c->kernel_launches = 0;
+    c->ev_used = 0;
+    return RADM2_OK;
+}
+
+int radm2_get_kernel_time(radm2_ctx *c, double *ms, int *launches)
+{
+    if (!valid_ctx(c) || !ms || !launches) return RADM2_E_ARG;
+    *ms = c->kernel_ms;
+    *launches = c->kernel_launches;
+    c->kernel_ms = 0.0;
+    c->kernel_launches = 0;
+    return RADM2_OK;
+}
+
+int radm2_get_ncell(const radm2_ctx *c) { return c ? c->ncell : RADM2_E_ARG; }
+
+size_t radm2_device_bytes(const radm2_ctx *c)
+{
+    if (!c) return 0;
+    return c->bytes + c->scratch_bytes + c->stage_bytes;
+}
+
+int radm2_selfcheck(void)
+{
+    // Layout bounds of every solver variant (host arithmetic only, no device needed).
+    const int bad = solver_layout_check_fp64_static() | solver_layout_check_fp64_persistent() |
+                    solver_layout_check_fp32_static() | solver_layout_check_fp32_persistent();
+    return bad ? RADM2_E_STATE : RADM2_OK;
+}
+
+const char *radm2_version(void) { return "radm2-b200 1.0 sm_100a (fp64 | fp32-LU+IR) x (static | persistent)"; }
+
+// ---------------------------------------------------------------- mechanism kernels on host arrays
+
+static int mech_call(radm2_ctx *c, int n, int kind, int fp32, const double *V, const double *FIX, const double *RCT,
+                     double *out, double *G, double *X, int *sing)
+{
+    if (!valid_ctx(c) || n <= 0) return RADM2_E_ARG;
+    CK(cudaSetDevice(c->o.device));
+    const int ld = (n + 31) / 32 * 32;
+    double *dv = nullptr, *df = nullptr, *dr = nullptr, *dout = nullptr, *stage = nullptr;
+    int *ds = nullptr;
+    const size_t cap = (size_t)ld * NJVS;
+    cudaError_t e = cudaSuccess;
+    auto up = [&](const double *h, int m, double *d) {
+        if (e != cudaSuccess) return;
+        e = cudaMemcpyAsync(stage, h, sizeof(double) * n * m, cudaMemcpyHostToDevice, c->st);
+        if (e == cudaSuccess) e = launch_aos_to_soa(n, m, ld, stage, d, c->st);
+    };
+    auto down = [&](const double *d, int m, double *h) {
+        if (e != cudaSuccess) return;
+        e = launch_soa_to_aos(n, m, ld, d, stage, c->st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(h, stage, sizeof(double) * n * m, cudaMemcpyDeviceToHost, c->st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+    };
+    e = cudaMalloc((void **)&stage, sizeof(double) * cap);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&dout, sizeof(double) * cap);
+    if (kind < 2) {
+        if (e == cudaSuccess) e = cudaMalloc((void **)&dv, sizeof(double) * ld * NVAR);
+        if (e == cudaSuccess) e = cudaMalloc((void **)&df, sizeof(double) * ld * NFIX);
+        if (e == cudaSuccess) e = cudaMalloc((void **)&dr, sizeof(double) * ld * NREACT);
+        up(V, NVAR, dv);
+        up(FIX, NFIX, df);
+        up(RCT, NREACT, dr);
+        if (e == cudaSuccess) e = kind == 0 ? launch_fun(n, ld, dv, df, dr, dout, c->st) : launch_jac(n, ld, dv, df, dr, dout, c->st);
+        down(dout, kind == 0 ? NVAR : NJVS, out);
+    } else {
+        if (e == cudaSuccess) e = cudaMalloc((void **)&dv, sizeof(double) * ld * NVAR);
+        if (e == cudaSuccess) e = cudaMalloc((void **)&ds, sizeof(int) * ld);
+        up(G, NJVS, dout);
+        up(X, NVAR, dv);
+        if (e == cudaSuccess) e = launch_decomp_solve(n, ld, fp32, dout, dv, ds, c->st);
+        down(dout, NJVS, G);
+        down(dv, NVAR, X);
+        if (e == cudaSuccess) e = cudaMemcpy(sing, ds, sizeof(int) * n, cudaMemcpyDeviceToHost);
+    }
+    cudaFree(stage);
+    cudaFree(dout);
+    cudaFree(dv);
+    cudaFree(df);
+    cudaFree(dr);
+    cudaFree(ds);
+    if (e != cudaSuccess) return fail_cuda(c, e, "mechanism kernel");
+    return RADM2_OK;
+}
+
+int radm2_fun(radm2_ctx *c, int n, const double *V, const double *FIX, const double *RCT, double *VDOT)
+{
+    if (!V || !FIX || !RCT || !VDOT) return RADM2_E_ARG;
+    return mech_call(c, n, 0, 0, V, FIX, RCT, VDOT, nullptr, nullptr, nullptr);
+}
+
+int radm2_jac(radm2_ctx *c, int n, const double *V, const double *FIX, const double *RCT, double *JVS)
+{
+    if (!V || !FIX || !RCT || !JVS) return RADM2_E_ARG;
+    return mech_call(c, n, 1, 0, V, FIX, RCT, JVS, nullptr, nullptr, nullptr);
+}
+
+int radm2_decomp_solve(radm2_ctx *c, int n, int precision, double *G, double *X, int *sing)
+{
+    if (!G || !X || !sing || (precision != RADM2_PREC_FP64 && precision != RADM2_PREC_FP32LU)) return RADM2_E_ARG;
+    return mech_call(c, n, 2, precision == RADM2_PREC_FP32LU, nullptr, nullptr, nullptr, nullptr, G, X, sing);
+}
+
+}  // extern "C"

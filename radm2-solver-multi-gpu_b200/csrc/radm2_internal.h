@@ -1,0 +1,59 @@
+// Internal interfaces between the C ABI (radm2_capi.cu) and the kernel files.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "radm2_device.cuh"
+
+namespace radm2 {
+
+constexpr int REDUCE_BLOCKS = 296;  // 2 x 148 SMs
+
+// Aggregated outcome of one integration, produced on the device.
+struct RunResult {
+    long long nacc, nrej, nfail;
+    int worst, max_att;
+    double tmin, tmax, hmin;
+};
+
+cudaError_t launch_rconst(int n, int ld, const double *jv, const double *temp, const double *fix,
+                          const double *rcn2o5, double *rconst, cudaStream_t st);
+cudaError_t launch_aos_to_soa(int n, int m, int ld, const double *aos, double *soa, cudaStream_t st);
+cudaError_t launch_soa_to_aos(int n, int m, int ld, const double *soa, double *aos, cudaStream_t st);
+cudaError_t launch_fun(int n, int ld, const double *var, const double *fix, const double *rconst, double *vdot,
+                       cudaStream_t st);
+cudaError_t launch_jac(int n, int ld, const double *var, const double *fix, const double *rconst, double *jvs,
+                       cudaStream_t st);
+cudaError_t launch_decomp_solve(int n, int ld, int fp32, double *g, double *x, int *sing, cudaStream_t st);
+size_t reduce_partials_bytes();
+cudaError_t launch_reduce(int n, const int *status, const int *nacc, const int *nrej, const double *texit,
+                          const double *hexit, void *partials, RunResult *out, cudaStream_t st);
+
+// Static properties of one solver variant on the current device.
+struct SolverInfo {
+    int regs;           // registers per thread
+    int local_bytes;    // local (spill) bytes per thread
+    int blocks_per_sm;  // resident blocks per SM (registers and shared memory)
+    int global_words;   // global-scratch doubles per thread
+    int smem_bytes;     // dynamic shared memory per block
+};
+
+// Solver kernels: one launcher per (precision, schedule) file, variant key
+// bs * 64 + min_blocks * 4 + place (place: bit 0 = LU in shared memory, bit 1 = rate
+// constants and state in shared memory).
+inline int variant_key(int bs, int place, int min_blocks) { return bs * 64 + min_blocks * 4 + place; }
+cudaError_t launch_solver_fp64_static(const SolveArgs &a, int key, int grid, cudaStream_t st);
+cudaError_t launch_solver_fp64_persistent(const SolveArgs &a, int key, int grid, cudaStream_t st);
+cudaError_t launch_solver_fp32_static(const SolveArgs &a, int key, int grid, cudaStream_t st);
+cudaError_t launch_solver_fp32_persistent(const SolveArgs &a, int key, int grid, cudaStream_t st);
+cudaError_t solver_info_fp64_static(int key, SolverInfo *out);
+cudaError_t solver_info_fp64_persistent(int key, SolverInfo *out);
+cudaError_t solver_info_fp32_static(int key, SolverInfo *out);
+cudaError_t solver_info_fp32_persistent(int key, SolverInfo *out);
+// Host-side bounds check of every built variant's working-set layout (0 = all in bounds).
+int solver_layout_check_fp64_static();
+int solver_layout_check_fp64_persistent();
+int solver_layout_check_fp32_static();
+int solver_layout_check_fp32_persistent();
+
+}  // namespace radm2

@@ -1,0 +1,434 @@
+// The fused per-cell ROS-3 solver kernel.
+//
+// One thread integrates one grid cell at a time through the reference's whole
+// step loop -- time-loop mask and step clamp (mgpu.cu:1595-1614), Jacobian and
+// matrix preparation (mgpu.cu:1672-2652, 3128-3166), pivot-free LU
+// (mgpu.cu:2726-2780), the three ROS-3 stages (mgpu.cu:3595-3625, restored),
+// and the error norm / step-size controller (mgpu.cu:3168-3262) -- without
+// returning to the host between steps.
+//
+// Per-thread working set, three regions, each laid out word-major per block
+// (word w of thread t at base + w*BS + t, so every access is coalesced / bank-
+// conflict free and carries a compile-time offset):
+//   RCY  rate constants (156) and state Y (59)             FP64
+//   VEC  Fcn0, K1, K2, K3 and a temporary (5 x 59)          FP64, global scratch
+//   LU   the 659 LU slots                                   LUT (double or float)
+// PLACE selects shared memory for LU (bit 0) and RCY (bit 1); what is not in
+// shared memory lives in the global scratch slot of the thread.
+//
+// Schedules:
+//   static      one thread per cell, cell = global thread index (the plain method)
+//   persistent  a grid sized to the machine; each lane takes its next cell from a
+//               global queue (warp-aggregated atomics) as soon as its current cell
+//               finishes, optionally in a caller-given order (cost-sorted cells).
+//
+// LU precision: double (plain FP64) or float with FP64 iterative refinement, the
+// residual b - G x being formed in FP64 with a fresh Jacobian-vector product.
+#pragma once
+
+#include "radm2_device.cuh"
+
+namespace radm2 {
+
+enum { SCHED_STATIC = 0, SCHED_PERSISTENT = 1 };
+enum { PLACE_GLOBAL = 0, PLACE_LU_SMEM = 1, PLACE_RCY_SMEM = 2 };
+
+constexpr int RCY_WORDS = NREACT + NVAR;  // 215
+constexpr int RCY_RC = 0, RCY_Y = NREACT;
+constexpr int VEC_WORDS = 5 * NVAR;  // 295
+constexpr int VEC_F0 = 0, VEC_K1 = NVAR, VEC_K2 = 2 * NVAR, VEC_K3 = 3 * NVAR, VEC_TMP = 4 * NVAR;
+
+template <typename LUT>
+struct LuWords {  // LU slots expressed in double words
+    static constexpr int value = sizeof(LUT) == 8 ? NJVS : (NJVS + 1) / 2;
+};
+
+// Where each region of a thread's working set lives, in doubles from the block base
+// of its memory (global scratch block or dynamic shared memory); a thread's word w
+// of a region sits at base + (off + w) * BS + thread.
+template <typename LUT, int PLACE>
+struct Layout {
+    static constexpr bool rcy_smem = (PLACE & PLACE_RCY_SMEM) != 0;
+    static constexpr bool lu_smem = (PLACE & PLACE_LU_SMEM) != 0;
+    static constexpr int vec_off = 0;  // always global
+    static constexpr int rcy_off = rcy_smem ? 0 : VEC_WORDS;
+    static constexpr int lu_off = lu_smem ? (rcy_smem ? RCY_WORDS : 0) : VEC_WORDS + RCY_WORDS;
+    static constexpr int global_words = VEC_WORDS + (rcy_smem ? 0 : RCY_WORDS) + (lu_smem ? 0 : LuWords<LUT>::value);
+    static constexpr int smem_words = (rcy_smem ? RCY_WORDS : 0) + (lu_smem ? LuWords<LUT>::value : 0);
+};
+
+// Host-side bounds check of a layout for block size bs: every word of every region
+// of every thread lands inside its block's allocation.  Returns 0 when it holds.
+template <typename LUT, int PLACE>
+inline int layout_check(int bs)
+{
+    using L = Layout<LUT, PLACE>;
+    const long gcap = (long)L::global_words * bs, scap = (long)L::smem_words * bs;  // doubles per block
+    // last element touched, in doubles (LU in LUT units converted to doubles)
+    const long vec_last = (long)(L::vec_off + VEC_WORDS - 1) * bs + (bs - 1);
+    const long rcy_last = (long)(L::rcy_off + RCY_WORDS - 1) * bs + (bs - 1);
+    const long lu_last_elem = (long)L::lu_off * bs * (8 / (long)sizeof(LUT)) + (long)(NJVS - 1) * bs + (bs - 1);
+    const long lu_last = lu_last_elem * (long)sizeof(LUT) / 8;
+    int bad = 0;
+    bad |= vec_last >= gcap;
+    bad |= rcy_last >= (L::rcy_smem ? scap : gcap);
+    bad |= lu_last >= (L::lu_smem ? scap : gcap);
+    // regions must not overlap inside one memory
+    if (!L::rcy_smem) bad |= L::rcy_off < L::vec_off + VEC_WORDS;
+    if (!L::lu_smem) bad |= L::lu_off < L::rcy_off + RCY_WORDS;
+    if (L::lu_smem && L::rcy_smem) bad |= L::lu_off < RCY_WORDS;
+    return bad;
+}
+
+// ---------------------------------------------------------------- phases
+// Each phase is its own (non-inlined) function: the register allocator sees one
+// phase's live set at a time, and the RHS exists once in the instruction stream
+// although both Fcn0 and the stage-2 right-hand side use it.
+
+// dst = F(v): the RHS at state v (v and dst may alias; dst is written after v is read).
+template <int BS>
+__device__ __noinline__ void ph_fun(const double *v, const double *rc, double *dst, double fix0, double fix1)
+{
+#define V(i) v[(i) * BS]
+#define RC(r) rc[(r) * BS]
+#define FIX(k) ((k) == 0 ? fix0 : fix1)
+#define VDOT_OUT(i, e) dst[(i) * BS] = (e)
+#include "gen/radm2_fun.inc"
+#undef VDOT_OUT
+#undef V
+#undef RC
+#undef FIX
+}
+
+// G = -J(y) + ghinv I in the LU slots (mgpu.cu:3139-3142 with the diagonal of 2700 restored).
+template <int BS, typename LUT>
+__device__ __noinline__ void ph_jac(const double *y, const double *rc, LUT *sg, double fix0, double fix1, double ghinv)
+{
+#define V(i) y[(i) * BS]
+#define RC(r) rc[(r) * BS]
+#define FIX(k) ((k) == 0 ? fix0 : fix1)
+#define G(s) sg[(s) * BS]
+#define JAC_OUT(s, e) G(s) = (LUT)(-(e))
+#define JAC_OUT_DIAG(s, e) G(s) = (LUT)((-(e)) + ghinv)
+#define JAC_OUT_ZERO(s, d) G(s) = (d) ? (LUT)((-0.0) + ghinv) : (LUT)(-0.0)
+#include "gen/radm2_jac.inc"
+#undef JAC_OUT
+#undef JAC_OUT_DIAG
+#undef JAC_OUT_ZERO
+#undef G
+#undef V
+#undef RC
+#undef FIX
+}
+
+// In-place LU; returns 0 or the 1-based row of a zero pivot (checked before the row is
+// eliminated, as mgpu.cu:2753-2757 does).
+template <int BS, typename LUT>
+__device__ __noinline__ int ph_decomp(LUT *sg)
+{
+    int sing = 0;
+#define G(s) sg[(s) * BS]
+#define LU_T LUT
+// One elimination step's loads may not be hoisted above the previous step: this bounds
+// the live set to one pivot row's worth of U entries and keeps the LU free of spills.
+#define LU_STEP_FENCE asm volatile("" ::: "memory")
+#define LU_PIVOT_CHECK(k, v) \
+    if (sing == 0 && (v) == (LUT)0) sing = (k) + 1
+#include "gen/radm2_decomp.inc"
+#undef LU_PIVOT_CHECK
+#undef LU_STEP_FENCE
+#undef LU_T
+#undef G
+    return sing;
+}
+
+// One ROS-3 stage: build the right-hand side, solve with the factored G, store K[stage].
+//   stage 0: Fcn0                      (mgpu.cu:3601-3602)
+//   stage 1: F(Y + A21 K1) + C21/h K1  (stage 2 reuses that F, NewF = 0; its partial
+//            right-hand side F + C31/h K1 is parked in K3)
+//   stage 2: (F + C31/h K1) + C32/h K2
+// FP64 LU: one substitution.  FP32 LU: the substitution in float, then `refine`
+// sweeps of x += G32^-1 (b - G64 x), residual in FP64 (G64 x = ghinv x - J x).
+template <int BS, typename LUT>
+__device__ __noinline__ void ph_stage(int stage, const double *y, const double *rc, double *vec, const LUT *sg,
+                                      double fix0, double fix1, double hc21, double hc31, double hc32,
+                                      double ghinv, int refine)
+{
+#define VW(w) vec[(w) * BS]
+#define G(s) sg[(s) * BS]
+    double x[NVAR];
+    if (stage == 0) {
+#pragma unroll
+        for (int i = 0; i < NVAR; i++) x[i] = VW(VEC_F0 + i);
+    } else if (stage == 1) {
+#pragma unroll
+        for (int i = 0; i < NVAR; i++) VW(VEC_TMP + i) = y[i * BS] + RADM2_ROS_A0 * VW(VEC_K1 + i);
+        ph_fun<BS>(vec + VEC_TMP * BS, rc, vec + VEC_TMP * BS, fix0, fix1);
+#pragma unroll
+        for (int i = 0; i < NVAR; i++) {
+            const double f = VW(VEC_TMP + i), k1 = VW(VEC_K1 + i);
+            x[i] = f + k1 * hc21;
+            VW(VEC_K3 + i) = f + k1 * hc31;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < NVAR; i++) x[i] = VW(VEC_K3 + i) + VW(VEC_K2 + i) * hc32;
+    }
+    if (sizeof(LUT) == 8) {
+#define X(i) x[i]
+#include "gen/radm2_solve.inc"
+#undef X
+    } else {
+        float xf[NVAR];
+#pragma unroll
+        for (int i = 0; i < NVAR; i++) {
+            VW(VEC_TMP + i) = x[i];
+            xf[i] = (float)x[i];
+        }
+#define X(i) xf[i]
+#include "gen/radm2_solve.inc"
+#undef X
+#pragma unroll
+        for (int i = 0; i < NVAR; i++) x[i] = (double)xf[i];
+        double *kout = vec + (VEC_K1 + stage * NVAR) * BS;
+#pragma unroll 1
+        for (int sweep = 0; sweep < refine; sweep++) {
+            // park x in the stage's output slot so the residual reads it from memory
+#pragma unroll
+            for (int i = 0; i < NVAR; i++) kout[i * BS] = x[i];
+            {
+#define V(i) y[(i) * BS]
+#define RC(r) rc[(r) * BS]
+#define FIX(k) ((k) == 0 ? fix0 : fix1)
+#define XIN(i) kout[(i) * BS]
+#define JX_OUT(row, e) xf[row] = (float)(VW(VEC_TMP + (row)) - (ghinv * kout[(row) * BS] - (e)))
+#include "gen/radm2_jacvec.inc"
+#undef JX_OUT
+#undef XIN
+#undef V
+#undef RC
+#undef FIX
+            }
+#define X(i) xf[i]
+#include "gen/radm2_solve.inc"
+#undef X
+#pragma unroll
+            for (int i = 0; i < NVAR; i++) x[i] = kout[i * BS] + (double)xf[i];
+        }
+    }
+    double *kout = vec + (VEC_K1 + stage * NVAR) * BS;
+#pragma unroll
+    for (int i = 0; i < NVAR; i++) kout[i * BS] = x[i];
+#undef VW
+#undef G
+}
+
+// Optional per-phase cycle counters (build with -DRADM2_PHASE_CLOCKS): lane 0 of every
+// warp adds clock64() deltas per phase into phase_clocks[warp][8]; profiling only.
+#ifdef RADM2_PHASE_CLOCKS
+__device__ unsigned long long phase_clocks[1 << 16][8];
+#define PCLK_DECL long long pclk_t = clock64();
+#define PCLK(ph)                                                                                   \
+    do {                                                                                           \
+        const long long t_ = clock64();                                                            \
+        if ((threadIdx.x & 31) == 0)                                                               \
+            phase_clocks[(blockIdx.x * BS + threadIdx.x) >> 5 & 0xffff][ph] += (unsigned long long)(t_ - pclk_t); \
+        pclk_t = t_;                                                                               \
+    } while (0)
+#else
+#define PCLK_DECL
+#define PCLK(ph) do { } while (0)
+#endif
+
+template <int BS, typename LUT, int SCHED, int PLACE, int MINB>
+__global__ void __launch_bounds__(BS, MINB) k_rosenbrock(const SolveArgs a)
+{
+    using L = Layout<LUT, PLACE>;
+    extern __shared__ double smem[];
+    double *const gblk = a.scratch + (size_t)blockIdx.x * (L::global_words * BS);  // block bases
+    double *const sblk = smem;
+    double *const vec = gblk + L::vec_off * BS + threadIdx.x;
+    double *const rcy = (L::rcy_smem ? sblk : gblk) + L::rcy_off * BS + threadIdx.x;
+    LUT *const sg = reinterpret_cast<LUT *>((L::lu_smem ? sblk : gblk) + L::lu_off * BS) + threadIdx.x;
+#define RW(w) rcy[(w) * BS]
+#define VW(w) vec[(w) * BS]
+#define G(s) sg[(s) * BS]
+    const SolveParams &P = a.p;
+    const int ld = a.ld;
+    const int dir = P.direction;
+
+    // ---- lane state
+    int cell;
+    if (SCHED == SCHED_STATIC) {
+        cell = blockIdx.x * BS + threadIdx.x;
+    } else {
+        const unsigned m = __activemask();
+        const int lane = threadIdx.x & 31;
+        const int leader = __ffs(m) - 1;
+        int base = 0;
+        if (lane == leader) base = atomicAdd(a.queue, __popc(m));
+        base = __shfl_sync(m, base, leader);
+        cell = base + __popc(m & ((1u << lane) - 1));
+    }
+    bool have = cell < a.ncell;
+    bool outer = true;  // next action: time-loop test, step clamp, Fcn0
+    bool done = false;  // cell finished (ok or error) and must be written back
+    int cidx = 0;       // cell index after the optional permutation
+    double T = 0.0, H = 0.0, fix0 = 0.0, fix1 = 0.0, hfirst = 0.0;
+    int rlast = 0, rmore = 0, nacc = 0, nrej = 0, nstp = 0, status = 1;
+
+    auto load_cell = [&](int c) {
+        cidx = (SCHED == SCHED_PERSISTENT && a.order) ? a.order[c] : c;
+        const double *v = a.var + cidx;
+#pragma unroll
+        for (int i = 0; i < NVAR; i++) RW(RCY_Y + i) = v[(size_t)i * ld];
+        const double *rc = a.rconst + cidx;
+#pragma unroll
+        for (int r = 0; r < NREACT; r++) RW(RCY_RC + r) = rc[(size_t)r * ld];
+        fix0 = a.fix[cidx];
+        fix1 = a.fix[(size_t)ld + cidx];
+        T = P.Tstart;
+        double hs = P.Hstart;
+        if (a.h0) {
+            const double h = a.h0[cidx];
+            if (h > 0.0 && h <= P.Hmax) hs = h;  // non-finite or out of range: default
+        }
+        H = mind(hs, P.Hmax);  // mgpu.cu:3475-3477
+        if (absd(H) <= 10.0 * P.Roundoff) H = DELTA_MIN;
+        rlast = rmore = nacc = nrej = nstp = 0;
+        status = 1;
+        hfirst = 0.0;
+        outer = true;
+        done = false;
+    };
+    auto store_cell = [&]() {
+        double *v = a.var + cidx;
+#pragma unroll
+        for (int i = 0; i < NVAR; i++) v[(size_t)i * ld] = RW(RCY_Y + i);
+        a.status[cidx] = status;
+        a.nacc[cidx] = nacc;
+        a.nrej[cidx] = nrej;
+        a.hfirst[cidx] = hfirst;
+        a.hexit[cidx] = H;
+        a.texit[cidx] = T;
+    };
+    auto next_cell = [&]() {
+        if (SCHED == SCHED_STATIC) {
+            have = false;
+            return;
+        }
+        const unsigned m = __activemask();
+        const int lane = threadIdx.x & 31;
+        const int leader = __ffs(m) - 1;
+        int base = 0;
+        if (lane == leader) base = atomicAdd(a.queue, __popc(m));
+        base = __shfl_sync(m, base, leader);
+        cell = base + __popc(m & ((1u << lane) - 1));
+        have = cell < a.ncell;
+        if (have) load_cell(cell);
+    };
+
+    if (have) load_cell(cell);
+    PCLK_DECL
+
+    for (;;) {
+        // Bring every lane that still has work to the start of a step attempt.
+        while (have && (outer || done)) {
+            if (done) {
+                store_cell();
+                next_cell();
+                continue;
+            }
+            // Time-loop mask (mgpu.cu:1608-1613).
+            const bool more = (dir > 0 && (T - P.Tend) + P.Roundoff <= 0.0) ||
+                              (dir < 0 && (P.Tend - T) + P.Roundoff <= 0.0);
+            if (!more) {
+                done = true;
+                continue;
+            }
+            H = mind(H, absd(P.Tend - T));
+            // Fcn0 = F(Y)
+            ph_fun<BS>(rcy + RCY_Y * BS, rcy + RCY_RC * BS, vec + VEC_F0 * BS, fix0, fix1);
+            outer = false;
+        }
+        PCLK(0);  // outer: cell load/store, time-loop test, Fcn0
+        if (!__any_sync(0xffffffffu, have)) break;
+        if (!have) continue;
+
+        // ---------------------------------------------------------------- one attempt
+        if (nstp >= P.max_steps) {
+            status = -6;
+            done = true;
+            continue;
+        }
+        if ((T + 0.1 * H == T) || (H <= P.Roundoff)) {
+            status = -7;
+            done = true;
+            continue;
+        }
+        const double ghinv = 1.0 / (dir * H * RADM2_ROS_GAMMA0);
+        // G = -J(Y) + ghinv I, written straight into the LU slots; then factor it.
+        ph_jac<BS, LUT>(rcy + RCY_Y * BS, rcy + RCY_RC * BS, sg, fix0, fix1, ghinv);
+        PCLK(1);
+        const int sing = ph_decomp<BS, LUT>(sg);
+        PCLK(2);
+        if (sing) {
+            status = -8;
+            done = true;
+            continue;
+        }
+        const double hc21 = RADM2_ROS_C0 / (dir * H);
+        const double hc31 = RADM2_ROS_C1 / (dir * H);
+        const double hc32 = RADM2_ROS_C2 / (dir * H);
+
+#pragma unroll 1
+        for (int stage = 0; stage < 3; stage++) {
+            ph_stage<BS, LUT>(stage, rcy + RCY_Y * BS, rcy + RCY_RC * BS, vec, sg, fix0, fix1, hc21, hc31, hc32, ghinv,
+                              a.refine);
+            PCLK(3 + stage);
+        }
+        nstp++;
+
+        // Error norm and step control (mgpu.cu:3223-3260).
+        double err = 0.0;
+#pragma unroll
+        for (int i = 0; i < NVAR; i++) {
+            const double k0 = VW(VEC_K1 + i), k1 = VW(VEC_K2 + i), k2 = VW(VEC_K3 + i);
+            const double y = RW(RCY_Y + i);
+            const double ynew = P.M[0] * k0 + P.M[1] * k1 + P.M[2] * k2 + y;
+            const double yerr = P.E[0] * k0 + P.E[1] * k1 + P.E[2] * k2;
+            const double ymax = maxd(absd(y), absd(ynew));
+            const double scale = P.AbsTol[i] + P.RelTol[i] * ymax;
+            err += (yerr * yerr) / (scale * scale);
+            VW(VEC_TMP + i) = ynew;
+        }
+        err = sqrt(err / (double)NVAR);
+        const double fac = mind(P.FacMax, maxd(P.FacMin, P.FacSafe / pow(err, 1.0 / RADM2_ROS_ELO)));
+        double hnew = H * fac;
+        if (err != err) hnew = H * P.FacRej;  // non-finite norm: shrink hard and retry
+        if ((err <= 1.0) || (H <= P.Hmin)) {
+#pragma unroll
+            for (int i = 0; i < NVAR; i++) RW(RCY_Y + i) = VW(VEC_TMP + i);
+            T += dir * H;
+            if (rlast) hnew = mind(hnew, H);
+            rlast = 0;
+            rmore = 0;
+            if (nacc == 0) hfirst = H;
+            nacc++;
+            H = hnew;
+            outer = true;
+        } else {
+            if (rmore) hnew = H * P.FacRej;
+            rmore = rlast;
+            rlast = 1;
+            nrej++;
+            H = hnew;
+        }
+        PCLK(6);  // error norm and step control
+    }
+#undef RW
+#undef VW
+#undef G
+}
+
+}  // namespace radm2

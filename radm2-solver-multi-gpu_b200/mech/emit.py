@@ -1,0 +1,501 @@
+#!/usr/bin/env python3
+"""Emit C / CUDA code for the RADM2 mechanism from mech/radm2_mech.json.
+
+Two consumers, one mechanism table:
+
+  csrc/gen/   fragments for the sm_100a kernels.  Each fragment is the body of
+              a device function and talks to its caller only through accessor
+              macros (V(i), RC(r), FIX(k), G(s), X(i), ...), so one fragment
+              serves the FP64 kernel, the FP32-LU kernel and the test kernels,
+              each with its own storage (registers, shared or global SoA).
+              The LU decomposition and the solves are fully unrolled to the
+              659-slot fill pattern.
+
+  oracle/gen/ plain C functions for the CPU oracle (rates, RHS, Jacobian) and
+              the CSR tables its table-driven LU / solve loops walk.
+
+Expressions are rendered fully parenthesised from the parse trees, so both
+sides evaluate every rate, RHS sum and Jacobian slot in the reference's own
+association order (mgpu.cu:763-918, 1103-1385, 1685-2652).
+
+Usage:  python emit.py      (reads radm2_mech.json beside this file)
+"""
+import json
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.dirname(HERE)
+REPO = os.path.dirname(PKG)
+CSRC_GEN = os.path.join(PKG, "csrc", "gen")
+ORACLE_GEN = os.path.join(REPO, "oracle", "gen")
+
+BANNER = ("/* Generated by radm2-solver-multi-gpu_b200/mech/emit.py from mech/radm2_mech.json\n"
+          " * (the RADM2 mechanism as encoded in the reference's mgpu.cu).  Do not edit. */\n")
+
+# Rate-law helpers: reference name -> this project's implementation name.
+CALLS = {"ARR2": "rk_arr2", "TROE": "rk_troe", "TROEE": "rk_troee",
+         "THERMAL_T2": "rk_thermal_t2", "k46": "rk_k46", "pow": "pow", "exp": "exp"}
+
+
+def lit(text):
+    """Render a numeric literal as a C double literal with the same value."""
+    if all(c.isdigit() for c in text):
+        return text + ".0"
+    return text
+
+
+class Renderer:
+    """Render an expression tree; `names` maps (array, index) / variables to C text."""
+
+    def __init__(self, ref, var):
+        self.ref = ref
+        self.var = var
+
+    def __call__(self, t):
+        k = t[0]
+        if k == "num":
+            return lit(t[1])
+        if k == "var":
+            return self.var(t[1])
+        if k == "ref":
+            return self.ref(t[1], t[2])
+        if k == "neg":
+            return "(-" + self(t[1]) + ")"
+        if k == "bin":
+            return "(" + self(t[2]) + " " + t[1] + " " + self(t[3]) + ")"
+        if k == "call":
+            return CALLS[t[1]] + "(" + ", ".join(self(a) for a in t[2]) + ")"
+        raise ValueError(k)
+
+
+def count_flops(t):
+    k = t[0]
+    if k in ("num", "var", "ref"):
+        return 0
+    if k == "neg":
+        return count_flops(t[1])
+    if k == "bin":
+        return 1 + count_flops(t[2]) + count_flops(t[3])
+    if k == "call":
+        return sum(count_flops(a) for a in t[2])
+    raise ValueError(k)
+
+
+def is_zero(t):
+    return t[0] == "num" and float(t[1]) == 0.0
+
+
+def load(path=os.path.join(HERE, "radm2_mech.json")):
+    with open(path) as f:
+        return json.load(f)
+
+
+
+# The reference's Jacobian keeps reaction 33 (H2O2 + OH) in the H2O2 row although its RHS
+# drops it: JVS[49] (row 13, col 13) has -B[43] = -k33 [OH], JVS[51] (13, 52) has
+# -B[44] = -k33 [H2O2].
+QUIRK_ROW, QUIRK_R, QUIRK_OH = 13, 33, 52
+
+# LU scheduling fence spacing, in loads of U entries (see the decomposition emitter).
+LU_FENCE_LOADS = int(os.environ.get("RADM2_LU_FENCE_LOADS", "48"))
+
+
+def deriv(t):
+    """Directional derivative of a rate expression along XIN (product rule over V factors)."""
+    k = t[0]
+    if k in ("num", "var"):
+        return None
+    if k == "ref":
+        return ["ref", "XIN", t[2]] if t[1] == "V" else None
+    if k == "bin" and t[1] == "*":
+        da, db = deriv(t[2]), deriv(t[3])
+        parts = []
+        if da is not None:
+            parts.append(["bin", "*", da, t[3]])
+        if db is not None:
+            parts.append(["bin", "*", t[2], db])
+        if not parts:
+            return None
+        return parts[0] if len(parts) == 1 else ["bin", "+", parts[0], parts[1]]
+    raise ValueError("rate expression not a product: %r" % (t,))
+
+
+def subst_a(t, rx):
+    """Replace A[rx] by da<rx> in an RHS term."""
+    if t[0] == "ref" and t[1] == "A":
+        assert t[2] == rx
+        return ["ref", "DA", rx]
+    if t[0] == "bin":
+        return ["bin", t[1], subst_a(t[2], rx), subst_a(t[3], rx)]
+    if t[0] == "neg":
+        return ["neg", subst_a(t[1], rx)]
+    return t
+
+
+def _eval(t, env):
+    k = t[0]
+    if k == "num":
+        return float(t[1])
+    if k == "ref":
+        return env[t[1]][t[2]]
+    if k == "neg":
+        return -_eval(t[1], env)
+    if k == "bin":
+        a, b = _eval(t[2], env), _eval(t[3], env)
+        if t[1] == "+":
+            return a + b
+        if t[1] == "-":
+            return a - b
+        if t[1] == "*":
+            return a * b
+        return a / b
+    raise ValueError(k)
+
+
+def check_jacvec(m, chains, uses):
+    """J_reference x (B partials, JVS slots, CSR) == directional-derivative form, on random data."""
+    import random
+    rnd = random.Random(7)
+    lu = m["lu"]
+    for _ in range(3):
+        env = {"V": [rnd.uniform(0.5, 2.0) for _ in range(59)], "F": [rnd.uniform(0.5, 2.0) for _ in range(2)],
+               "RCT": [rnd.uniform(0.5, 2.0) for _ in range(156)], "XIN": [rnd.uniform(-1, 1) for _ in range(59)]}
+        env["B"] = {}
+        for k, bt in m["bvals"].items():
+            env["B"][int(k)] = _eval(bt, env)
+        ref = [0.0] * 59
+        for sl, t in enumerate(m["jvs"]):
+            ref[lu["irow"][sl]] += _eval(t, env) * env["XIN"][lu["icol"][sl]]
+        env["DA"] = {}
+        for rx, t in enumerate(m["rates"]):
+            d = deriv(t)
+            env["DA"][rx] = _eval(d, env) if d is not None else 0.0
+        got = [0.0] * 59
+        for rx, lst in sorted(uses.items()):
+            for (i, pos, op, term) in lst:
+                v = _eval(subst_a(term, rx), env)
+                got[i] = v if pos == 0 else (got[i] + v if op == "+" else got[i] - v)
+        R = env["RCT"][QUIRK_R]
+        got[QUIRK_ROW] -= R * env["V"][QUIRK_OH] * env["XIN"][QUIRK_ROW] + R * env["V"][QUIRK_ROW] * env["XIN"][QUIRK_OH]
+        for i in range(59):
+            assert abs(got[i] - ref[i]) <= 1e-9 * (1 + abs(ref[i])), (i, got[i], ref[i])
+
+
+# ----------------------------------------------------------------------------- CUDA fragments
+
+def kernel_ref(arr, i):
+    return {"RCT": "RC(%d)", "V": "V(%d)", "F": "FIX(%d)", "A": "a%d", "B": "b%d",
+            "jv": "JV(%d)", "XIN": "XIN(%d)", "DA": "da%d"}[arr] % i
+
+
+def kernel_var(name):
+    return {"TEMP": "TEMP", "C_M": "C_M", "rc_n2o5": "RC_N2O5"}[name]
+
+
+def emit_cuda(m, out_dir):
+    os.makedirs(out_dir, exist_ok=True)
+    r = Renderer(kernel_ref, kernel_var)
+    sz = m["sizes"]
+    lu = m["lu"]
+    crow, diag, icol = lu["crow"], lu["diag"], lu["icol"]
+    nvar = sz["NVAR"]
+    flops = {}
+
+    # --- header with sizes, tables and method coefficients
+    h = [BANNER, "#pragma once\n"]
+    for k in ("NVAR", "NFIX", "NREACT", "LU_NONZERO", "NPH", "NB"):
+        h.append("#define RADM2_%s %d\n" % (k, sz[k]))
+    h.append("#define RADM2_NJV_USED 21   /* photolysis rates 0..20 feed RCONST 0..20 */\n")
+    ros = m["ros3"]
+    for name, key in (("A", "ros_A"), ("C", "ros_C"), ("M", "ros_M"), ("E", "ros_E"),
+                      ("ALPHA", "ros_Alpha"), ("GAMMA", "ros_Gamma")):
+        for i, v in enumerate(ros[key]):
+            h.append("#define RADM2_ROS_%s%d %s\n" % (name, i, lit(v)))
+    h.append("#define RADM2_ROS_ELO %s\n" % lit(ros["ros_ELO"]))
+    h.append("\n/* LU pattern (CSR over the 659 slots), recovered from mgpu.cu:2873-3090 */\n")
+    h.append("#define RADM2_LU_CROW_INIT {%s}\n" % ",".join(map(str, crow)))
+    h.append("#define RADM2_LU_DIAG_INIT {%s}\n" % ",".join(map(str, diag)))
+    h.append("#define RADM2_LU_ICOL_INIT {%s}\n" % ",".join(map(str, icol)))
+    h.append("#define RADM2_LU_DIAG_SLOTS(X) %s\n" % " ".join("X(%d,%d)" % (i, d) for i, d in enumerate(diag)))
+    names = m["species"]
+    h.append("#define RADM2_SPECIES_NAMES_INIT {%s}\n" % ",".join('"%s"' % n for n in names[:nvar]))
+
+    # --- rate constants: RC_OUT(r, value)
+    body = [BANNER, "/* 156 rate constants, mgpu.cu:763-918.  Inputs: JV(k), TEMP, C_M, RC_N2O5. */\n"]
+    for i, t in enumerate(m["rconst"]):
+        body.append("RC_OUT(%d, %s);\n" % (i, r(t)))
+    write(os.path.join(out_dir, "radm2_rconst.inc"), body)
+
+    # --- RHS, reaction-major: each rate A_r is formed once and immediately added into
+    # the accumulators of the species it touches.  Every Vdot sum of the reference lists
+    # its reactions in increasing order, so accumulating in reaction order applies the
+    # same binary operations to each accumulator in the same order as the reference's
+    # left-to-right sum (bit-identical), while only 59 accumulators stay live.
+    body = [BANNER, "/* ODE right-hand side, mgpu.cu:1103-1385, reaction-major.  Inputs: RC(r), V(i), FIX(k).\n"
+            " * Output VDOT_OUT(i, value) after all reactions. */\n"]
+    f = 0
+    chains = []
+    for i, t in enumerate(m["vdot"]):
+        chain = []
+        node = t
+        while node[0] == "bin" and node[1] in "+-":
+            chain.append((node[1], node[3]))
+            node = node[2]
+        chain.append((None, node))
+        chain.reverse()
+        chains.append(chain)
+        f += count_flops(t)
+    uses = {}
+    for i, chain in enumerate(chains):
+        for pos, (op, term) in enumerate(chain):
+            rs = set()
+            def walk(x):
+                if x[0] == "ref" and x[1] == "A":
+                    rs.add(x[2])
+                elif x[0] == "bin":
+                    walk(x[2]); walk(x[3])
+                elif x[0] == "neg":
+                    walk(x[1])
+            walk(term)
+            assert len(rs) == 1, (i, term)
+            uses.setdefault(rs.pop(), []).append((i, pos, op, term))
+    for i in range(len(chains)):
+        body.append("double vd%d;\n" % i)
+    for rx, t in enumerate(m["rates"]):
+        f += count_flops(t)
+        if rx not in uses:
+            continue
+        body.append("{ const double a%d = %s;\n" % (rx, r(t)))
+        for (i, pos, op, term) in uses[rx]:
+            if pos == 0:
+                body.append("  vd%d = %s;\n" % (i, r(term)))
+            else:
+                body.append("  vd%d = (vd%d %s %s);\n" % (i, i, op, r(term)))
+        body.append("}\n")
+    for i in range(len(chains)):
+        body.append("VDOT_OUT(%d, vd%d);\n" % (i, i))
+    flops["fun"] = f
+    write(os.path.join(out_dir, "radm2_fun.inc"), body)
+
+    # --- Jacobian in LU slot order, partial-major: each partial B_b is formed once and
+    # added into the slots that use it.  Every JVS slot of the reference sums its
+    # partials in increasing b, so accumulating in b order applies the same operations
+    # to each slot in the same order (bit-identical); at most ~94 slots are open at once.
+    # JAC_OUT(s, value) / JAC_OUT_DIAG(s, value) when a slot is complete; literal-zero
+    # slots use JAC_OUT_ZERO(s, is_diag).
+    dset = set(diag)
+    body = [BANNER, "/* Sparse Jacobian in LU slot order, mgpu.cu:1685-2652, partial-major.\n"
+            " * Inputs: RC(r), V(i), FIX(k). */\n"]
+    f = 0
+    juses = {}
+    last_b = {}
+    for sl, t in enumerate(m["jvs"]):
+        if is_zero(t):
+            body.append("JAC_OUT_ZERO(%d%s);\n" % (sl, ", 1" if sl in dset else ", 0"))
+            continue
+        f += count_flops(t)
+        chain = []
+        node = t
+        while node[0] == "bin" and node[1] in "+-":
+            chain.append((node[1], node[3]))
+            node = node[2]
+        chain.append((None, node))
+        chain.reverse()
+        for pos, (op, term) in enumerate(chain):
+            bs = []
+
+            def walkb(x):
+                if x[0] == "ref" and x[1] == "B":
+                    bs.append(x[2])
+                elif x[0] == "bin":
+                    walkb(x[2]); walkb(x[3])
+                elif x[0] == "neg":
+                    walkb(x[1])
+            walkb(term)
+            assert len(bs) == 1, (sl, term)
+            juses.setdefault(bs[0], []).append((sl, pos, op, term, pos == len(chain) - 1))
+    for k in sorted(m["bvals"], key=int):
+        bt = m["bvals"][k]
+        f += count_flops(bt)
+        b = int(k)
+        if b not in juses:
+            continue
+        body.append("{ const double b%d = %s;\n" % (b, r(bt)))
+        for (sl, pos, op, term, is_last) in juses[b]:
+            if pos == 0:
+                expr = r(term)
+            else:
+                expr = "(js%d %s %s)" % (sl, op, r(term))
+            if is_last:
+                body.append("  %s(%d, %s);\n" % ("JAC_OUT_DIAG" if sl in dset else "JAC_OUT", sl, expr))
+            elif pos == 0:
+                body.append("  double js%d = %s;\n" % (sl, expr))
+            else:
+                body.append("  js%d = %s;\n" % (sl, expr))
+        body.append("}\n")
+    flops["jac"] = f
+    # declarations of the open accumulators must precede their first use: hoist them.
+    decl = sorted({int(x.split()[1][2:]) for x in body if x.startswith("  double js")})
+    body = [x.replace("  double js", "  js") for x in body]
+    body.insert(2, "".join("double js%d;\n" % sl for sl in decl))
+    write(os.path.join(out_dir, "radm2_jac.inc"), body)
+
+    # --- Jacobian-vector product J x for the FP64 residual of the FP32-LU refinement.
+    # RADM2's rates are products of rate constants and concentrations, so J x is the exact
+    # directional derivative of the RHS: dA_r = sum over its concentration factors of the
+    # product rule, accumulated reaction-major like the RHS (59 live accumulators).  The
+    # reference's Jacobian additionally keeps the H2O2 + OH loss in the H2O2 row that its
+    # RHS drops (mgpu.cu:1275 vs 2011, 2013); those two slots are added explicitly.
+    # check_jacvec() below verifies J_reference x == this on random data.
+    body = [BANNER, "/* y = J(V) x, J the mgpu.cu:1685-2652 Jacobian, as the directional derivative of\n"
+            " * the RHS plus the H2O2 row terms.  Inputs: RC, V, FIX, XIN(i).  Output JX_OUT(row, value). */\n"]
+    f = 0
+    for i in range(len(chains)):
+        body.append("double jx%d;\n" % i)
+    for rx, t in enumerate(m["rates"]):
+        if rx not in uses:
+            continue
+        dt = deriv(t)
+        f += count_flops(dt)
+        body.append("{ const double da%d = %s;\n" % (rx, r(dt)))
+        for (i, pos, op, term) in uses[rx]:
+            dterm = subst_a(term, rx)
+            f += count_flops(dterm)
+            if pos == 0:
+                body.append("  jx%d = %s;\n" % (i, r(dterm)))
+            else:
+                body.append("  jx%d = (jx%d %s %s);\n" % (i, i, op, r(dterm)))
+        body.append("}\n")
+    q = QUIRK_ROW
+    body.append("jx%d = ((jx%d - (RC(%d) * V(%d)) * XIN(%d)) - (RC(%d) * V(%d)) * XIN(%d));\n"
+                % (q, q, QUIRK_R, QUIRK_OH, q, QUIRK_R, q, QUIRK_OH))
+    for i in range(len(chains)):
+        body.append("JX_OUT(%d, jx%d);\n" % (i, i))
+    flops["jacvec"] = f + 6
+    write(os.path.join(out_dir, "radm2_jacvec.inc"), body)
+    check_jacvec(m, chains, uses)
+
+    # --- unrolled row-Doolittle LU (mgpu.cu:2746-2779 order) on G(s).
+    # LU_PIVOT_CHECK(k, value) sees the un-eliminated diagonal of row k (as the reference does).
+    body = [BANNER, "/* In-place pivot-free LU of G on the fixed fill pattern, the row-by-row\n"
+            " * elimination order of mgpu.cu:2746-2779, unrolled.  Accessors: G(s), LU_T (type),\n"
+            " * LU_PIVOT_CHECK(row, diag_value); LU_STEP_FENCE ends each elimination step\n"
+            " * (a compiler scheduling fence, or nothing). */\n"
+            "#ifndef LU_STEP_FENCE\n#define LU_STEP_FENCE do { } while (0)\n#endif\n"]
+    f = 0
+    since_fence = 0
+    for k in range(nvar):
+        body.append("{ /* row %d */\n" % k)
+        body.append("  LU_PIVOT_CHECK(%d, G(%d));\n" % (k, diag[k]))
+        if crow[k] == diag[k]:
+            body.append("}\n")  # no elimination, row unchanged
+            continue
+        for s in range(crow[k], crow[k + 1]):
+            body.append("  LU_T w%d = G(%d);\n" % (icol[s], s))
+        for kk in range(crow[k], diag[k]):
+            j = icol[kk]
+            body.append("  { const LU_T a = -w%d / G(%d); w%d = -a;\n" % (j, diag[j], j))
+            f += 1
+            for jj in range(diag[j] + 1, crow[j + 1]):
+                body.append("    w%d += a * G(%d);\n" % (icol[jj], jj))
+                f += 2
+            # A fence once LU_FENCE_LOADS loads have been issued since the last one: the
+            # scheduler may overlap that many loads but no more (bounds the live set).
+            since_fence += crow[j + 1] - diag[j]
+            if since_fence >= LU_FENCE_LOADS:
+                body.append("  LU_STEP_FENCE;\n")
+                since_fence = 0
+            body.append("  }\n")
+        for s in range(crow[k], crow[k + 1]):
+            body.append("  G(%d) = w%d;\n" % (s, icol[s]))
+        body.append("}\n")
+    flops["decomp"] = f
+    write(os.path.join(out_dir, "radm2_decomp.inc"), body)
+
+    # --- unrolled forward (unit lower) and backward (upper / diag) solves, mgpu.cu:2873-3090.
+    body = [BANNER, "/* Solve (LU) x = b in place on X(i), mgpu.cu:2873-3090 order.  Accessors: G(s), X(i). */\n"]
+    f = 0
+    for k in range(nvar):
+        if crow[k] == diag[k]:
+            continue
+        expr = "X(%d)" % k
+        for s in range(crow[k], diag[k]):
+            expr = "(%s - G(%d) * X(%d))" % (expr, s, icol[s])
+            f += 2
+        body.append("X(%d) = %s;\n" % (k, expr))
+    for k in reversed(range(nvar)):
+        expr = "X(%d)" % k
+        for s in range(diag[k] + 1, crow[k + 1]):
+            expr = "(%s - G(%d) * X(%d))" % (expr, s, icol[s])
+            f += 2
+        body.append("X(%d) = %s / G(%d);\n" % (k, expr, diag[k]))
+        f += 1
+    flops["solve"] = f
+    write(os.path.join(out_dir, "radm2_solve.inc"), body)
+
+    h.append("\n/* Algorithmic flop counts per call, counted from the emitted expressions */\n")
+    for k, v in sorted(flops.items()):
+        h.append("#define RADM2_FLOPS_%s %d\n" % (k.upper(), v))
+    write(os.path.join(out_dir, "radm2_gen.h"), h)
+    return flops
+
+
+# ----------------------------------------------------------------------------- oracle C
+
+def oracle_ref(arr, i):
+    return {"RCT": "RCT[%d]", "V": "V[%d]", "F": "F[%d]", "A": "A[%d]", "B": "B[%d]",
+            "jv": "jv[%d]"}[arr] % i
+
+
+def oracle_var(name):
+    return {"TEMP": "TEMP", "C_M": "C_M", "rc_n2o5": "rc_n2o5"}[name]
+
+
+def emit_oracle(m, out_dir):
+    os.makedirs(out_dir, exist_ok=True)
+    r = Renderer(oracle_ref, oracle_var)
+    sz = m["sizes"]
+    lu = m["lu"]
+    c = [BANNER, '#include "../radm2_oracle.h"\n#include <math.h>\n\n']
+    c.append("/* LU pattern tables (CSR), recovered from mgpu.cu:2873-3090 */\n")
+    c.append("const int orc_lu_crow[%d] = {%s};\n" % (len(lu["crow"]), ",".join(map(str, lu["crow"]))))
+    c.append("const int orc_lu_diag[%d] = {%s};\n" % (len(lu["diag"]), ",".join(map(str, lu["diag"]))))
+    c.append("const int orc_lu_icol[%d] = {%s};\n\n" % (len(lu["icol"]), ",".join(map(str, lu["icol"]))))
+    c.append("/* Rate constants: mgpu.cu:763-918 (dev_Update_RCONST) */\n")
+    c.append("void orc_rconst(const double *jv, double TEMP, double C_M, double rc_n2o5, double *RCT)\n{\n")
+    for i, t in enumerate(m["rconst"]):
+        c.append("  RCT[%d] = %s;\n" % (i, r(t)))
+    c.append("}\n\n")
+    c.append("/* ODE right-hand side: mgpu.cu:1103-1385 (dev_Fun) */\n")
+    c.append("void orc_fun(const double *V, const double *F, const double *RCT, double *Vdot)\n{\n")
+    c.append("  double A[%d];\n" % sz["NREACT"])
+    for i, t in enumerate(m["rates"]):
+        c.append("  A[%d] = %s;\n" % (i, r(t)))
+    for i, t in enumerate(m["vdot"]):
+        c.append("  Vdot[%d] = %s;\n" % (i, r(t)))
+    c.append("}\n\n")
+    c.append("/* Sparse Jacobian in LU slot order: mgpu.cu:1685-2652 (dev_Jac_SP) */\n")
+    c.append("void orc_jac(const double *V, const double *F, const double *RCT, double *JVS)\n{\n")
+    c.append("  double B[%d];\n" % sz["NB"])
+    for k in sorted(m["bvals"], key=int):
+        c.append("  B[%s] = %s;\n" % (k, r(m["bvals"][k])))
+    for s, t in enumerate(m["jvs"]):
+        c.append("  JVS[%d] = %s;\n" % (s, r(t)))
+    c.append("}\n")
+    write(os.path.join(out_dir, "radm2_oracle_gen.c"), c)
+
+
+def write(path, parts):
+    with open(path, "w") as f:
+        f.write("".join(parts))
+
+
+def main():
+    m = load()
+    flops = emit_cuda(m, CSRC_GEN)
+    emit_oracle(m, ORACLE_GEN)
+    print("emitted", CSRC_GEN, ORACLE_GEN, flops)
+
+
+if __name__ == "__main__":
+    main()
