@@ -375,12 +375,29 @@ def emit_cuda(m, out_dir):
     write(os.path.join(out_dir, "radm2_jacvec.inc"), body)
     check_jacvec(m, chains, uses)
 
-    # --- unrolled row-Doolittle LU (mgpu.cu:2746-2779 order) on G(s).
-    # LU_PIVOT_CHECK(k, value) sees the un-eliminated diagonal of row k (as the reference does).
+    for recip in (False, True):
+        fd, fs = emit_lu(crow, diag, icol, nvar, out_dir, recip)
+        if not recip:
+            flops["decomp"], flops["solve"] = fd, fs
+
+    h.append("\n/* Algorithmic flop counts per call, counted from the emitted expressions */\n")
+    for k, v in sorted(flops.items()):
+        h.append("#define RADM2_FLOPS_%s %d\n" % (k.upper(), v))
+    write(os.path.join(out_dir, "radm2_gen.h"), h)
+    return flops
+
+
+def emit_lu(crow, diag, icol, nvar, out_dir, recip):
+    """Unrolled row-Doolittle LU (mgpu.cu:2746-2779 order) and the triangular solves
+    (mgpu.cu:2873-3090 order).  With recip, each finished row stores the reciprocal of
+    its pivot in the diagonal slot and the eliminations / back substitution multiply by
+    it (one division per row instead of one per lower entry and per solve row)."""
+    sfx = "_rcp" if recip else ""
     body = [BANNER, "/* In-place pivot-free LU of G on the fixed fill pattern, the row-by-row\n"
             " * elimination order of mgpu.cu:2746-2779, unrolled.  Accessors: G(s), LU_T (type),\n"
             " * LU_PIVOT_CHECK(row, diag_value); LU_STEP_FENCE ends each elimination step\n"
-            " * (a compiler scheduling fence, or nothing). */\n"
+            " * (a compiler scheduling fence, or nothing).%s */\n"
+            % ("\n * Reciprocal form: the diagonal slots hold 1/U(k,k) on exit." if recip else ""),
             "#ifndef LU_STEP_FENCE\n#define LU_STEP_FENCE do { } while (0)\n#endif\n"]
     f = 0
     since_fence = 0
@@ -388,13 +405,19 @@ def emit_cuda(m, out_dir):
         body.append("{ /* row %d */\n" % k)
         body.append("  LU_PIVOT_CHECK(%d, G(%d));\n" % (k, diag[k]))
         if crow[k] == diag[k]:
+            if recip:
+                body.append("  G(%d) = (LU_T)1 / G(%d);\n" % (diag[k], diag[k]))
+                f += 1
             body.append("}\n")  # no elimination, row unchanged
             continue
-        for s in range(crow[k], crow[k + 1]):
-            body.append("  LU_T w%d = G(%d);\n" % (icol[s], s))
+        for sl in range(crow[k], crow[k + 1]):
+            body.append("  LU_T w%d = G(%d);\n" % (icol[sl], sl))
         for kk in range(crow[k], diag[k]):
             j = icol[kk]
-            body.append("  { const LU_T a = -w%d / G(%d); w%d = -a;\n" % (j, diag[j], j))
+            if recip:
+                body.append("  { const LU_T a = -w%d * G(%d); w%d = -a;\n" % (j, diag[j], j))
+            else:
+                body.append("  { const LU_T a = -w%d / G(%d); w%d = -a;\n" % (j, diag[j], j))
             f += 1
             for jj in range(diag[j] + 1, crow[j + 1]):
                 body.append("    w%d += a * G(%d);\n" % (icol[jj], jj))
@@ -406,38 +429,36 @@ def emit_cuda(m, out_dir):
                 body.append("  LU_STEP_FENCE;\n")
                 since_fence = 0
             body.append("  }\n")
-        for s in range(crow[k], crow[k + 1]):
-            body.append("  G(%d) = w%d;\n" % (s, icol[s]))
+        for sl in range(crow[k], crow[k + 1]):
+            if recip and sl == diag[k]:
+                body.append("  G(%d) = (LU_T)1 / w%d;\n" % (sl, icol[sl]))
+                f += 1
+            else:
+                body.append("  G(%d) = w%d;\n" % (sl, icol[sl]))
         body.append("}\n")
-    flops["decomp"] = f
-    write(os.path.join(out_dir, "radm2_decomp.inc"), body)
+    write(os.path.join(out_dir, "radm2_decomp%s.inc" % sfx), body)
+    fdec = f
 
-    # --- unrolled forward (unit lower) and backward (upper / diag) solves, mgpu.cu:2873-3090.
-    body = [BANNER, "/* Solve (LU) x = b in place on X(i), mgpu.cu:2873-3090 order.  Accessors: G(s), X(i). */\n"]
+    body = [BANNER, "/* Solve (LU) x = b in place on X(i), mgpu.cu:2873-3090 order.  Accessors: G(s), X(i).%s */\n"
+            % (" Diagonal slots hold reciprocals." if recip else "")]
     f = 0
     for k in range(nvar):
         if crow[k] == diag[k]:
             continue
         expr = "X(%d)" % k
-        for s in range(crow[k], diag[k]):
-            expr = "(%s - G(%d) * X(%d))" % (expr, s, icol[s])
+        for sl in range(crow[k], diag[k]):
+            expr = "(%s - G(%d) * X(%d))" % (expr, sl, icol[sl])
             f += 2
         body.append("X(%d) = %s;\n" % (k, expr))
     for k in reversed(range(nvar)):
         expr = "X(%d)" % k
-        for s in range(diag[k] + 1, crow[k + 1]):
-            expr = "(%s - G(%d) * X(%d))" % (expr, s, icol[s])
+        for sl in range(diag[k] + 1, crow[k + 1]):
+            expr = "(%s - G(%d) * X(%d))" % (expr, sl, icol[sl])
             f += 2
-        body.append("X(%d) = %s / G(%d);\n" % (k, expr, diag[k]))
+        body.append("X(%d) = %s %s G(%d);\n" % (k, expr, "*" if recip else "/", diag[k]))
         f += 1
-    flops["solve"] = f
-    write(os.path.join(out_dir, "radm2_solve.inc"), body)
-
-    h.append("\n/* Algorithmic flop counts per call, counted from the emitted expressions */\n")
-    for k, v in sorted(flops.items()):
-        h.append("#define RADM2_FLOPS_%s %d\n" % (k.upper(), v))
-    write(os.path.join(out_dir, "radm2_gen.h"), h)
-    return flops
+    write(os.path.join(out_dir, "radm2_solve%s.inc" % sfx), body)
+    return fdec, f
 
 
 # ----------------------------------------------------------------------------- oracle C
