@@ -309,8 +309,10 @@ def main():
             tr = json.load(f)
         key = "%s-%s" % (args.precision, args.schedule)
         if key in tr:
-            # DRAM bytes per cell-step from an ncu capture, scaled to one full launch
-            traffic = tr[key]["bytes_per_cell_step"] * ncell
+            # DRAM bytes per step attempt from one ncu capture (small case), scaled to the
+            # attempts of an average launch here: traffic grows with attempts, not cells
+            att = (tot["n_accepted"] + tot["n_rejected"]) / max(klaunch, 1)
+            traffic = tr[key]["dram_bytes_per_attempt"] * att
     line = {
         "metric": "chem cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": el_ms / args.steps,

@@ -195,8 +195,10 @@ inline double maxh(double a, double b) { return (a >= b) ? a : b; }
 inline double minh(double b, double c) { return (b < c) ? b : c; }
 inline double absh(double x) { return (x >= 0) ? x : -x; }
 
+}  // namespace
+
 // IPAR/RPAR parsing and validation, mgpu.cu:3684-3811 (same checks, same order, same codes).
-int parse_params(double Tstart, double Tend, const double *AbsTol, const double *RelTol, const double *RPAR,
+int radm2::parse_params(double Tstart, double Tend, const double *AbsTol, const double *RelTol, const double *RPAR,
                  const int *IPAR, int float_coeffs, SolveParams *p, int *autonomous)
 {
     static const double ros_M[3] = {RADM2_ROS_M0, RADM2_ROS_M1, RADM2_ROS_M2};
@@ -240,6 +242,8 @@ int parse_params(double Tstart, double Tend, const double *AbsTol, const double 
     p->direction = (Tend >= Tstart) ? +1 : -1;
     return 1;
 }
+
+namespace {
 
 int key_of(const radm2_ctx *c, int bs)
 {
@@ -346,11 +350,12 @@ int enqueue_integration(radm2_ctx *c, const SolveParams &p, int slot, int bs, in
             CK(cudaEventCreate(&e));
             c->ev.push_back(e);
         }
-        CK(cudaEventRecord(c->ev[2 * slot], c->st));
+        // External flag: under stream capture the record becomes a graph node (re-recorded per replay).
+        CK(cudaEventRecordWithFlags(c->ev[2 * slot], c->st, cudaEventRecordExternal));
     }
     CK(launch_solver(c, a, bs, grid));
     if (c->timing) {
-        CK(cudaEventRecord(c->ev[2 * slot + 1], c->st));
+        CK(cudaEventRecordWithFlags(c->ev[2 * slot + 1], c->st, cudaEventRecordExternal));
         if (slot + 1 > c->ev_used) c->ev_used = slot + 1;
     }
     CK(launch_reduce(c->ncell, c->status, c->nacc, c->nrej, c->texit, c->hexit, c->partials, c->d_res + slot, c->st));

@@ -16,6 +16,11 @@ struct RunResult {
     double tmin, tmax, hmin;
 };
 
+// IPAR/RPAR parsing with the reference's checks and codes (mgpu.cu:3684-3811): returns 1
+// or a negative IERR; fills p and the autonomous flag.
+int parse_params(double Tstart, double Tend, const double *AbsTol, const double *RelTol, const double *RPAR,
+                 const int *IPAR, int float_coeffs, SolveParams *p, int *autonomous);
+
 cudaError_t launch_rconst(int n, int ld, const double *jv, const double *temp, const double *fix,
                           const double *rcn2o5, double *rconst, cudaStream_t st);
 cudaError_t launch_aos_to_soa(int n, int m, int ld, const double *aos, double *soa, cudaStream_t st);
