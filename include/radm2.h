@@ -193,6 +193,34 @@ size_t radm2_device_bytes(const radm2_ctx *ctx);
  * working-set offsets inside its allocation, for every built variant). */
 int radm2_selfcheck(void);
 
+/*
+ * Integration without any device allocation, for callers that cannot call cudaMalloc:
+ * code that runs while a CUDA graph is being captured (allocation fails under capture),
+ * host frameworks that reserved all device memory for their own pool at start-up, and
+ * real-time couplings whose memory budget is fixed at initialisation.  No counterpart in
+ * the reference (which allocates inside Rosenbrock(), mgpu.cu:3444-3468).
+ *
+ * Same method, IPAR/RPAR meaning and return codes as radm2_rosenbrock, but without a
+ * context: inputs and outputs are the caller's device arrays in struct-of-arrays layout
+ * with leading dimension ld (var[59][ld] species in/out, fix[2][ld], temp[ld],
+ * rc_n2o5[ld] or NULL, jv[28][ld]), on the current device and the given cudaStream_t
+ * (NULL = default stream); status[ncell] (device, or NULL) receives each cell's outcome.
+ * Everything else -- rate constants, the solver's scratch, per-cell bookkeeping -- lives
+ * in one statically sized device array of RADM2_NOALLOC_BYTES (64 MiB) that every GPU
+ * which loads the library holds until the process exits.  Limits: ncell <= ld <=
+ * RADM2_NOALLOC_MAX_CELLS; larger sizes return RADM2_E_TOOBIG (split the batch).
+ * The first call on a device looks up the array's device address (set-up); make that
+ * first call before any stream capture.  All calls share the array, so calls that
+ * overlap on the GPU (other streams, other host threads) race: serialise them.  The
+ * call blocks until the integration has finished.  Calls no allocating routine.
+ */
+#define RADM2_NOALLOC_MAX_CELLS 32768
+#define RADM2_NOALLOC_BYTES (64u << 20)
+int radm2_rosenbrock_noalloc(int ncell, int ld, double *var, const double *fix, const double *temp,
+                             const double *rc_n2o5, const double *jv, double Tstart, double Tend,
+                             const double *AbsTol, const double *RelTol, double *RPAR, int *IPAR, int *status,
+                             void *stream);
+
 /* Library build string (arch, variants). */
 const char *radm2_version(void);
 

@@ -71,6 +71,9 @@ SIGNATURES = {
     "radm2_fma_peak": (ctypes.c_int, [ctypes.c_int, _D, _D]),
     "radm2_get_ncell": (ctypes.c_int, [ctypes.c_void_p]),
     "radm2_device_bytes": (ctypes.c_size_t, [ctypes.c_void_p]),
+    "radm2_rosenbrock_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                                 ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double,
+                                                 ctypes.c_double, _D, _D, _D, _I, ctypes.c_void_p, ctypes.c_void_p]),
     "radm2_selfcheck": (ctypes.c_int, []),
     "radm2_version": (ctypes.c_char_p, []),
 }
