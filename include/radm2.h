@@ -189,6 +189,40 @@ int radm2_fma_peak(int device, double *fp64_tflops, double *fp32_tflops);
 int radm2_get_ncell(const radm2_ctx *ctx);
 size_t radm2_device_bytes(const radm2_ctx *ctx);
 
+/*
+ * Learned step seeding.  A small network (84 state features -> 3 x 128 GELU -> 2, BF16
+ * weights on the tensor cores with FP32 accumulation, FP32 master weights, Adam) predicts
+ * each cell's starting step h0 and accepted-step count from its state.  The predictions
+ * seed radm2_set_cell_hstart-style starting steps (the Rosenbrock error controller still
+ * accepts or rejects every step; non-finite or out-of-range predictions fall back to the
+ * default Hstart) and a descending-cost visiting order for the persistent schedule.
+ * Features per cell: log10 of the 59 species (floor 1e-3), T, log10 M, log10 H2O,
+ * log10(J_k + 1e-12) for the 21 photolysis rates in use, and dt.  Outputs are
+ * standardised log10 h0 and log10(accepted steps + 1).
+ */
+typedef struct radm2_mlp radm2_mlp;
+int radm2_mlp_nparams(void);
+int radm2_mlp_create(radm2_mlp **mlp, int device, unsigned int seed);
+int radm2_mlp_destroy(radm2_mlp *mlp);
+int radm2_mlp_set_params(radm2_mlp *mlp, const float *params);   /* host, radm2_mlp_nparams() floats */
+int radm2_mlp_get_params(radm2_mlp *mlp, float *params);
+/* Feature (84) and output (2) standardisation. */
+int radm2_mlp_set_norm(radm2_mlp *mlp, const float *xmean, const float *xstd, const float *ymean, const float *ystd);
+/* Standardised outputs y[n][2] for features x[n][84] (host arrays). */
+int radm2_mlp_forward(radm2_mlp *mlp, int n, const float *x, float *y);
+/* Gradient of the mean squared error over n samples (host arrays), without an update. */
+int radm2_mlp_gradients(radm2_mlp *mlp, int n, const float *x, const float *target, float *grad, float *loss);
+/* One Adam step on a batch in device memory: x[n][84], target[n][2] (standardised). */
+int radm2_mlp_train_step(radm2_mlp *mlp, int n, const float *x, const float *target, float lr, float *loss);
+int radm2_mlp_synchronize(radm2_mlp *mlp);
+/* Safety factor on seeded starting steps: h0 = scale * predicted step (default 1). */
+int radm2_mlp_set_h0_scale(radm2_mlp *mlp, float scale);
+/* Features of the context's current cell states, host out[ncell][84]. */
+int radm2_get_features(radm2_ctx *ctx, double dt, float *out);
+/* Seed the context from the network: per-cell starting steps (set_h0) and the
+ * descending-predicted-cost cell order of the persistent schedule (set_order). */
+int radm2_seed_cells(radm2_ctx *ctx, radm2_mlp *mlp, double dt, int set_h0, int set_order);
+
 /* Host-only consistency check of the library's kernel layouts (every thread's
  * working-set offsets inside its allocation, for every built variant). */
 int radm2_selfcheck(void);

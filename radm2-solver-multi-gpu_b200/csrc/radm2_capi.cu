@@ -12,41 +12,7 @@
 
 using namespace radm2;
 
-struct radm2_ctx {
-    radm2_opts o{};
-    int nsm = 0;
-    cudaStream_t own = nullptr;
-    cudaStream_t st = nullptr;
-    int ncell = 0, ld = 0;
-    double *var = nullptr, *fix = nullptr, *temp = nullptr, *rcn = nullptr, *jv = nullptr, *rconst = nullptr;
-    bool have_rcn = false;
-    bool rconst_valid = false;
-    double *h0 = nullptr;
-    int *order = nullptr;
-    int *status = nullptr, *nacc = nullptr, *nrej = nullptr;
-    double *hfirst = nullptr, *hexit = nullptr, *texit = nullptr;
-    int *queue = nullptr;  // one counter per split
-    int queue_cap = 0;
-    double *scratch = nullptr;
-    size_t scratch_bytes = 0;
-    double *stage = nullptr;
-    size_t stage_bytes = 0;
-    void *partials = nullptr;
-    RunResult *d_res = nullptr, *h_res = nullptr;
-    int res_cap = 0;
-    size_t bytes = 0;
-    std::string err;
-    radm2_stats stats{};
-    // cached split graph
-    cudaGraphExec_t gexec = nullptr;
-    std::vector<unsigned char> gkey;
-    // solver-kernel timing
-    bool timing = false;
-    std::vector<cudaEvent_t> ev;  // start/stop pairs, one per result slot
-    int ev_used = 0;
-    double kernel_ms = 0.0;
-    int kernel_launches = 0;
-};
+#include "radm2_ctx.h"
 
 namespace {
 
@@ -315,8 +281,8 @@ SolveArgs make_args(radm2_ctx *c, const SolveParams &p, int *queue)
     a.var = c->var;
     a.fix = c->fix;
     a.rconst = c->rconst;
-    a.h0 = c->h0;
-    a.order = c->order;
+    a.h0 = c->use_h0 ? c->h0 : nullptr;
+    a.order = c->use_order ? c->order : nullptr;
     a.queue = queue;
     a.scratch = c->scratch;
     a.status = c->status;
@@ -426,6 +392,8 @@ bool valid_ctx(const radm2_ctx *c) { return c != nullptr; }
 
 }  // namespace
 
+void radm2::ctx_drop_graph(radm2_ctx *c) { drop_graph(c); }
+
 extern "C" {
 
 int radm2_opts_default(radm2_opts *o)
@@ -487,6 +455,9 @@ int radm2_destroy(radm2_ctx *c)
     drop_graph(c);
     free_cells(c);
     for (cudaEvent_t e : c->ev) cudaEventDestroy(e);
+    cudaFree(c->seed_keys);
+    cudaFree(c->seed_idx);
+    cudaFree(c->seed_tmp);
     if (c->scratch) cudaFree(c->scratch);
     if (c->stage) cudaFree(c->stage);
     if (c->partials) cudaFree(c->partials);
@@ -746,6 +717,7 @@ int radm2_set_cell_hstart(radm2_ctx *c, const double *h0)
     }
     if (!c->h0) CK(cudaMalloc((void **)&c->h0, sizeof(double) * c->ld));
     CK(cudaMemcpyAsync(c->h0, h0, sizeof(double) * c->ncell, cudaMemcpyHostToDevice, c->st));
+    c->use_h0 = true;
     return RADM2_OK;
 }
 
@@ -770,6 +742,7 @@ int radm2_set_cell_order(radm2_ctx *c, const int *order)
     if (!c->order) CK(cudaMalloc((void **)&c->order, sizeof(int) * c->ld));
     CK(cudaMemcpyAsync(c->order, order, sizeof(int) * c->ncell, cudaMemcpyHostToDevice, c->st));
     CK(cudaStreamSynchronize(c->st));
+    c->use_order = true;
     return RADM2_OK;
 }
 

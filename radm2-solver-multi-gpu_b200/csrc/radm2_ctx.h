@@ -1,0 +1,56 @@
+// The context behind the opaque radm2_ctx handle (shared by radm2_capi.cu and radm2_mlp.cu).
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "../../include/radm2.h"
+#include "radm2_internal.h"
+
+struct radm2_ctx {
+    radm2_opts o{};
+    int nsm = 0;
+    cudaStream_t own = nullptr;
+    cudaStream_t st = nullptr;
+    int ncell = 0, ld = 0;
+    double *var = nullptr, *fix = nullptr, *temp = nullptr, *rcn = nullptr, *jv = nullptr, *rconst = nullptr;
+    bool have_rcn = false;
+    bool rconst_valid = false;
+    double *h0 = nullptr;
+    int *order = nullptr;
+    int *status = nullptr, *nacc = nullptr, *nrej = nullptr;
+    double *hfirst = nullptr, *hexit = nullptr, *texit = nullptr;
+    int *queue = nullptr;  // one counter per split
+    int queue_cap = 0;
+    double *scratch = nullptr;
+    size_t scratch_bytes = 0;
+    double *stage = nullptr;
+    size_t stage_bytes = 0;
+    void *partials = nullptr;
+    radm2::RunResult *d_res = nullptr, *h_res = nullptr;
+    int res_cap = 0;
+    size_t bytes = 0;
+    std::string err;
+    radm2_stats stats{};
+    // cached split graph
+    cudaGraphExec_t gexec = nullptr;
+    std::vector<unsigned char> gkey;
+    // solver-kernel timing
+    bool timing = false;
+    std::vector<cudaEvent_t> ev;  // start/stop pairs, one per result slot
+    int ev_used = 0;
+    double kernel_ms = 0.0;
+    int kernel_launches = 0;
+    // learned seeding work arrays (radm2_seed_cells)
+    unsigned int *seed_keys = nullptr;
+    int *seed_idx = nullptr;
+    void *seed_tmp = nullptr;
+    size_t seed_tmp_bytes = 0;
+    int seed_cap = 0;
+    bool use_h0 = true, use_order = true;  // whether the solver reads h0 / order when set
+};
+
+namespace radm2 {
+// Drop a cached split graph (its baked-in arguments changed).
+void ctx_drop_graph(radm2_ctx *c);
+}  // namespace radm2

@@ -23,6 +23,8 @@ LIB_PATH = os.path.join(os.path.dirname(_HERE), "libradm2_b200.so")
 
 _D = ctypes.POINTER(ctypes.c_double)
 _I = ctypes.POINTER(ctypes.c_int)
+_F = ctypes.POINTER(ctypes.c_float)
+NFEAT = 84
 
 
 class Opts(ctypes.Structure):
@@ -69,6 +71,21 @@ SIGNATURES = {
     "radm2_set_kernel_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "radm2_get_kernel_time": (ctypes.c_int, [ctypes.c_void_p, _D, _I]),
     "radm2_fma_peak": (ctypes.c_int, [ctypes.c_int, _D, _D]),
+    "radm2_mlp_nparams": (ctypes.c_int, []),
+    "radm2_mlp_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_uint]),
+    "radm2_mlp_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "radm2_mlp_set_params": (ctypes.c_int, [ctypes.c_void_p, _F]),
+    "radm2_mlp_get_params": (ctypes.c_int, [ctypes.c_void_p, _F]),
+    "radm2_mlp_set_norm": (ctypes.c_int, [ctypes.c_void_p, _F, _F, _F, _F]),
+    "radm2_mlp_forward": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _F, _F]),
+    "radm2_mlp_gradients": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _F, _F, _F, _F]),
+    "radm2_mlp_train_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                            ctypes.c_float, _F]),
+    "radm2_mlp_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
+    "radm2_mlp_set_h0_scale": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_float]),
+    "radm2_get_features": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, _F]),
+    "radm2_seed_cells": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_int,
+                                        ctypes.c_int]),
     "radm2_get_ncell": (ctypes.c_int, [ctypes.c_void_p]),
     "radm2_device_bytes": (ctypes.c_size_t, [ctypes.c_void_p]),
     "radm2_rosenbrock_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
@@ -276,6 +293,15 @@ class Solver:
     def device_bytes(self):
         return int(self.lib.radm2_device_bytes(self.h))
 
+    # ---- learned seeding
+    def features(self, dt):
+        out = np.empty((self.ncell, NFEAT), dtype=np.float32)
+        self._check(self.lib.radm2_get_features(self.h, dt, out.ctypes.data_as(_F)))
+        return out
+
+    def seed_cells(self, mlp, dt, h0=True, order=True):
+        self._check(self.lib.radm2_seed_cells(self.h, mlp.h, dt, 1 if h0 else 0, 1 if order else 0))
+
     # ---- mechanism kernels
     def fun(self, V, FIX, RCT):
         n = V.shape[0]
@@ -297,3 +323,76 @@ class Solver:
         sing = np.empty(n, np.int32)
         self._check(self.lib.radm2_decomp_solve(self.h, n, precision, _dp(G), _dp(X), _ip(sing)))
         return G, X, sing
+
+
+class Mlp:
+    """The step-seeding network (radm2_mlp_* in the C ABI)."""
+
+    def __init__(self, seed=0, device=0):
+        self.lib = load()
+        h = ctypes.c_void_p()
+        rc = self.lib.radm2_mlp_create(ctypes.byref(h), device, seed)
+        if rc != 0:
+            raise RadmError(rc, self.lib.radm2_error_string(rc).decode())
+        self.h = h
+        self.nparams = self.lib.radm2_mlp_nparams()
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.radm2_mlp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != 0:
+            raise RadmError(rc, self.lib.radm2_error_string(rc).decode())
+
+    @staticmethod
+    def _f(a, shape=None):
+        a = np.ascontiguousarray(a, dtype=np.float32)
+        return a.reshape(shape) if shape is not None else a
+
+    def params(self):
+        out = np.empty(self.nparams, dtype=np.float32)
+        self._check(self.lib.radm2_mlp_get_params(self.h, out.ctypes.data_as(_F)))
+        return out
+
+    def set_params(self, p):
+        p = self._f(p, (self.nparams,))
+        self._check(self.lib.radm2_mlp_set_params(self.h, p.ctypes.data_as(_F)))
+
+    def set_norm(self, xmean, xstd, ymean, ystd):
+        a = [self._f(v) for v in (xmean, xstd, ymean, ystd)]
+        self._check(self.lib.radm2_mlp_set_norm(self.h, *[v.ctypes.data_as(_F) for v in a]))
+        self.norm = a
+
+    def forward(self, x):
+        x = self._f(x, (-1, NFEAT))
+        y = np.empty((x.shape[0], 2), dtype=np.float32)
+        self._check(self.lib.radm2_mlp_forward(self.h, x.shape[0], x.ctypes.data_as(_F), y.ctypes.data_as(_F)))
+        return y
+
+    def gradients(self, x, t):
+        x, t = self._f(x, (-1, NFEAT)), self._f(t, (-1, 2))
+        g = np.empty(self.nparams, dtype=np.float32)
+        loss = ctypes.c_float()
+        self._check(self.lib.radm2_mlp_gradients(self.h, x.shape[0], x.ctypes.data_as(_F), t.ctypes.data_as(_F),
+                                                 g.ctypes.data_as(_F), ctypes.byref(loss)))
+        return g, loss.value
+
+    def train_step(self, n, x_dev_ptr, t_dev_ptr, lr, want_loss=False):
+        loss = ctypes.c_float()
+        self._check(self.lib.radm2_mlp_train_step(self.h, n, ctypes.c_void_p(x_dev_ptr), ctypes.c_void_p(t_dev_ptr),
+                                                  lr, ctypes.byref(loss) if want_loss else None))
+        return loss.value if want_loss else None
+
+    def synchronize(self):
+        self._check(self.lib.radm2_mlp_synchronize(self.h))
+
+    def set_h0_scale(self, scale):
+        self._check(self.lib.radm2_mlp_set_h0_scale(self.h, scale))

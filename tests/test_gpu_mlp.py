@@ -1,0 +1,90 @@
+"""The step-seeding network: GPU forward/backward kernels against the CPU FP64 reference
+(oracle/mlp_ref.py, with bfloat16 rounding emulated where the tensor cores take bf16
+operands), training on the GPU, and what the trained network gains."""
+import numpy as np
+import pytest
+
+import mlp_ref
+import radm2b200
+from radm2b200 import inputs, seeding
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def feats():
+    cells = inputs.make_cells(2048, 11, "mixed")
+    with radm2b200.Solver() as s:
+        s.set_cells(cells)
+        x = s.features(600.0)
+    return x
+
+
+def _net(x, seed=3):
+    net = radm2b200.Mlp(seed=seed)
+    xm, xs = x.mean(0), np.where(x.std(0) > 1e-6, x.std(0), 1.0)
+    net.set_norm(xm, xs, np.zeros(2), np.ones(2))
+    return net, xm.astype(np.float32), xs.astype(np.float32)
+
+
+def test_features_are_finite_and_shaped(feats):
+    assert feats.shape == (2048, 84) and np.isfinite(feats).all()
+    assert (feats[:, 83] == 600.0).all()
+
+
+def test_forward_matches_reference(feats):
+    net, xm, xs = _net(feats)
+    p = net.params()
+    y = net.forward(feats[:1000])
+    yr, _, _ = mlp_ref.forward_backward(p, xm, xs, feats[:1000], bf=True)
+    assert np.abs(y - yr).max() < 1e-2 * max(1.0, np.abs(yr).max())
+
+
+def test_gradients_match_reference(feats):
+    net, xm, xs = _net(feats)
+    p = net.params()
+    t = np.random.default_rng(1).normal(size=(1000, 2)).astype(np.float32)
+    g, loss = net.gradients(feats[:1000], t)
+    _, loss_r, g_r = mlp_ref.forward_backward(p, xm, xs, feats[:1000], t, bf=True)
+    _, loss_e, g_e = mlp_ref.forward_backward(p, xm, xs, feats[:1000], t, bf=False)
+    assert abs(loss - loss_r) <= 1e-3 * loss_r
+    o = 0
+    for name, n in mlp_ref.SIZES:
+        a, b, c = g[o:o + n], g_r[o:o + n], g_e[o:o + n]
+        o += n
+        # same bf16 rounding points: FP32 vs FP64 accumulation only
+        assert np.linalg.norm(a - b) <= 2e-2 * np.linalg.norm(b) + 1e-9, name
+        # against the exact FP64 network: bounded by bf16 quantisation of operands
+        assert np.linalg.norm(a - c) <= 1e-1 * np.linalg.norm(c) + 1e-9, name
+
+
+def test_training_reduces_loss_and_gains_steps():
+    """Train on traces of one seed, evaluate on a disjoint seed: seeded starting steps must
+    cut the step attempts of the same integration, and the answers stay as accurate as the
+    unseeded method's against an FP64 oracle run at rtol 1e-8 (checked on a subset)."""
+    import oracle
+    X, Y = seeding.generate_traces(32768, 3, seed=101)
+    net, hist = seeding.fit(X, Y, epochs=12, batch=1024, lr=3e-3)
+    assert hist[-1] < 0.5 * hist[0] or hist[-1] < 0.2
+    cells = inputs.make_cells(8192, 102, "mixed")
+    y0, t0, _, _ = seeding.evaluate_split_loop(cells, 3, net=None)
+    y1, t1, _, _ = seeding.evaluate_split_loop(cells, 3, net=net, safety=0.5)
+    att0, att1 = t0["acc"] + t0["rej"], t1["acc"] + t1["rej"]
+    print("attempts default %d learned %d (accepted %d -> %d, rejected %d -> %d)"
+          % (att0, att1, t0["acc"], t1["acc"], t0["rej"], t1["rej"]))
+    assert att1 < att0
+    # accuracy against a tight oracle on 96 cells: the seeded run is no worse than the default
+    idx = np.arange(0, 8192, 86)[:96]
+    with radm2b200.Solver() as s:
+        s.set_cells(cells)
+        rc = s.get_rconst()[idx]
+    ipar, rpar = radm2b200.default_params(hstart=6.0)
+    ok, p = oracle.params(0.0, 600.0, np.ones(59), np.full(59, 1e-8), rpar, ipar)
+    yt = cells["VAR"][idx]
+    for _ in range(3):
+        yt, _ = oracle.integrate(yt, cells["FIX"][idx], rc, p)
+    above = np.abs(yt) > 1.0
+    e0 = (np.abs(y0[idx] - yt)[above] / np.abs(yt)[above]).max()
+    e1 = (np.abs(y1[idx] - yt)[above] / np.abs(yt)[above]).max()
+    print("max rel err vs rtol-1e-8 oracle: default %.2e learned %.2e" % (e0, e1))
+    assert e1 <= 1.5 * e0 + 1e-3
