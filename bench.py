@@ -2,18 +2,26 @@
 """Benchmark of the batched RADM2 ROS-3 chemistry solve on B200.
 
 Metric: chem cell-steps/s -- one cell advanced through one 600 s operator-split
-chemistry step.  A benchmark "step" is one such split over every cell of the
-workload (default: 1,048,576 cells, 30% night, plain FP64 method, the
-operator-split loop replayed as one CUDA graph).  K timed steps are K
-consecutive splits (K = 6 is one simulated hour).
+chemistry step, at rtol 1e-3 / atol 1 molec/cm^3.  A benchmark "step" is one such
+split over every cell of the workload; K timed steps are K consecutive splits
+replayed as one CUDA graph.
+
+Default: the 4,194,304-cell mixed-regime evaluation batch (20% urban, 40% remote,
+40% night, seed 3), method "learned": the FP64 persistent work-stealing solver with
+every split's starting steps seeded by the step-seeding network inside the graph
+(network trained first, untimed, on solver traces of a disjoint seed).  The same
+K splits are then run by the plain FP64 GPU solver (static cell-per-thread schedule,
+default Hstart) for the learned-vs-plain ratio, and both final states are compared
+with an FP64 rtol 1e-8 reference on a subset of cells.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload NAME] [--method learned|plain] [--precision fp64|fp32lu]
 
 N > 1 runs under torchrun, one process per GPU; each rank integrates its own
-contiguous shard of the global cell index space (weak scaling, no collective on
-the data path); time is the max over ranks.  `--impl reference` times the CPU
-restatement of the reference's per-cell Rosenbrock on the host cores (the
-reference itself does not build with CUDA 12.9) on a bounded sample.
+contiguous shard of the global cell index space (weak scaling, no collective on the
+data path); time is the max over ranks.  `--impl reference` times the CPU
+restatement of the reference's per-cell Rosenbrock (the reference itself does not
+build with CUDA 12.9) on the host cores, on a bounded sample of the same workload.
 """
 import argparse
 import json
@@ -35,14 +43,20 @@ FLOPS_PER_ATTEMPT = 1272 + 59 + 3588 + 3 * 1259 + 1085 + 24 * 59
 FLOPS_PER_ACCEPT = 1085
 # FP32-LU variant: each stage solve adds `refine` sweeps of Jv (880, FP64) + solve (1259) + 3 x 59.
 FLOPS_PER_SWEEP = 3 * (880 + 1259 + 3 * 59)
+# Kernels enqueued per split: solver + 2-pass statistics reduction; seeding adds features,
+# network forward and h0 write-back.
+LAUNCHES_PLAIN, LAUNCHES_SEED = 3, 3
 
 WORKLOADS = {
     # name: (cells per GPU, seed, generator workload, night fraction, dt)
+    "mixed-4m-eval": (4194304, 3, "mixed", 0.4, 600.0),  # learned evaluation batch (disjoint seed)
+    "mixed-4m": (4194304, 2, "mixed", 0.4, 600.0),       # batching configuration
     "plain-1m": (1048576, 1, "plain", 0.3, 600.0),
     "plain-4k": (4096, 0, "plain", 0.0, 600.0),
-    "plain-64k": (65536, 1, "plain", 0.3, 600.0),  # profiling case (same distributions as plain-1m)
-    "mixed-4m": (4194304, 2, "mixed", 0.4, 600.0),
+    "plain-64k": (65536, 1, "plain", 0.3, 600.0),        # profiling case (same distributions as plain-1m)
+    "mixed-256k": (262144, 3, "mixed", 0.4, 600.0),      # quick check of the default path
 }
+ATOL, RTOL, RTOL_TIGHT = 1.0, 1.0e-3, 1.0e-8
 
 
 def parse():
@@ -51,11 +65,14 @@ def parse():
     ap.add_argument("--steps", type=int, default=6)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="plain-1m", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="mixed-4m-eval", choices=sorted(WORKLOADS))
+    ap.add_argument("--method", default="learned", choices=["learned", "plain"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32lu"])
     ap.add_argument("--schedule", default="persistent", choices=["static", "persistent"])
     ap.add_argument("--block-threads", type=int, default=0)
     ap.add_argument("--blocks-per-sm", type=int, default=0)
+    ap.add_argument("--accuracy-cells", type=int, default=8192)
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain comparison arm")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -117,40 +134,45 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def flops_of(stats, precision, refine):
-    att = stats["n_accepted"] + stats["n_rejected"]
-    f = att * FLOPS_PER_ATTEMPT + stats["n_accepted"] * FLOPS_PER_ACCEPT
+def flops_of(acc, rej, precision, refine):
+    att = acc + rej
+    f = att * FLOPS_PER_ATTEMPT + acc * FLOPS_PER_ACCEPT
     if precision == "fp32lu":
         f += att * refine * FLOPS_PER_SWEEP
     return float(f)
 
 
-def cpu_baseline(cells, dt, target_s=12.0, nthreads=0):
-    """The oracle (CPU restatement of the reference's per-cell Rosenbrock) on a bounded sample."""
+def oracle_sample(cells, n, nsplit, dt, rtol, nthreads):
+    """Integrate the first n cells for nsplit consecutive splits with the CPU oracle.
+    Returns (final state, seconds of integration)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     import radm2b200
-    nthreads = nthreads or os.cpu_count() or 1
-    atol, rtol = np.ones(59), np.full(59, 1e-3)
     ipar, rpar = radm2b200.default_params(hstart=0.01 * dt)
-    ok, p = oracle.params(0.0, dt, atol, rtol, rpar, ipar)
-    rc_all = None
+    ok, p = oracle.params(0.0, dt, np.full(59, ATOL), np.full(59, rtol), rpar, ipar)
+    sl = slice(0, n)
+    rc = oracle.rconst(cells["JV"][sl], cells["TEMP"][sl], cells["FIX"][sl], cells["RC_N2O5"][sl], nthreads)
+    y = cells["VAR"][sl]
+    t = time.perf_counter()
+    for _ in range(nsplit):
+        y, _ = oracle.integrate(y, cells["FIX"][sl], rc, p, nthreads)
+    return y, time.perf_counter() - t
 
-    def run(n):
-        nonlocal rc_all
-        sl = slice(0, n)
-        rc = oracle.rconst(cells["JV"][sl], cells["TEMP"][sl], cells["FIX"][sl], cells["RC_N2O5"][sl], nthreads)
-        t = time.perf_counter()
-        oracle.integrate(cells["VAR"][sl], cells["FIX"][sl], rc, p, nthreads)
-        return time.perf_counter() - t
 
-    probe = min(len(cells["TEMP"]), max(256, 8 * nthreads))
-    tp = run(probe)
-    n = int(min(len(cells["TEMP"]), 65536, max(probe, probe * target_s / max(tp, 1e-3))))
-    t = run(n)
+def cpu_baseline(cells, dt, target_s=12.0):
+    """The oracle (CPU restatement of the reference's per-cell Rosenbrock) on a bounded
+    sample of the workload: all host cores (OpenMP over cells), and one core."""
+    nthreads = os.cpu_count() or 1
+    ncell = len(cells["TEMP"])
+    probe = min(ncell, max(512, 16 * nthreads))
+    _, tp = oracle_sample(cells, probe, 1, dt, RTOL, nthreads)
+    n = int(min(ncell, max(probe, probe * target_s / max(tp, 1e-3))))
+    _, t = oracle_sample(cells, n, 1, dt, RTOL, nthreads)
+    n1 = max(64, int(n / nthreads / 4))
+    _, t1 = oracle_sample(cells, n1, 1, dt, RTOL, 1)
     return {"value": n / t, "unit": "cell-steps/s", "cores": nthreads, "kind": "port",
             "sample": "first %d cells of the workload, one %g s split, %d OpenMP threads" % (n, dt, nthreads),
-            "seconds": t}
+            "seconds": t, "value_1core": n1 / t1, "sample_1core": "first %d cells, 1 thread" % n1}
 
 
 def run_reference(args):
@@ -159,27 +181,25 @@ def run_reference(args):
         return
     from radm2b200 import inputs
     ncell, seed, wl, night, dt = WORKLOADS[args.workload]
-    sample = min(ncell, 65536)
-    cells = inputs.make_cells(sample, seed, wl, night)
+    nthreads = os.cpu_count() or 1
+    probe_cells = inputs.make_cells(min(ncell, 1024), seed, wl, night)
+    _, tp = oracle_sample(probe_cells, len(probe_cells["TEMP"]), 1, dt, RTOL, nthreads)
+    per_cell = tp / len(probe_cells["TEMP"])
+    # each step ~8 s of work on this host: the first n cells of the workload
+    n = int(min(ncell, max(1024, 8.0 / max(per_cell, 1e-9))))
+    cells = inputs.make_cells(n, seed, wl, night)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     import radm2b200
-    nthreads = os.cpu_count() or 1
-    atol, rtol = np.ones(59), np.full(59, 1e-3)
     ipar, rpar = radm2b200.default_params(hstart=0.01 * dt)
-    ok, p = oracle.params(0.0, dt, atol, rtol, rpar, ipar)
+    ok, p = oracle.params(0.0, dt, np.full(59, ATOL), np.full(59, RTOL), rpar, ipar)
     rc = oracle.rconst(cells["JV"], cells["TEMP"], cells["FIX"], cells["RC_N2O5"], nthreads)
-    # size each step to ~8 s of work on this host
-    t = time.perf_counter()
-    oracle.integrate(cells["VAR"][:512], cells["FIX"][:512], rc[:512], p, nthreads)
-    per_cell = (time.perf_counter() - t) / 512
-    n = int(min(sample, max(512, 8.0 / max(per_cell, 1e-9))))
-    y = cells["VAR"][:n]
+    y = cells["VAR"]
     for _ in range(args.warmup):
-        y, _ = oracle.integrate(y, cells["FIX"][:n], rc[:n], p, nthreads)
+        oracle.integrate(y, cells["FIX"], rc, p, nthreads)
     t = time.perf_counter()
     for _ in range(args.steps):
-        y, _ = oracle.integrate(y, cells["FIX"][:n], rc[:n], p, nthreads)
+        y, _ = oracle.integrate(y, cells["FIX"], rc, p, nthreads)
     el = time.perf_counter() - t
     v = n * args.steps / el
     line = {"impl": "reference", "metric": "chem cell-steps/s", "value": v, "unit": "cell-steps/s",
@@ -192,6 +212,19 @@ def run_reference(args):
                                        (n, args.workload, args.steps, dt)},
             "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def rel_errors(y, ref):
+    """Relative errors of y against ref on entries above atol, and on entries where the
+    relative tolerance governs the error control (|ref| >= atol / rtol)."""
+    out = {}
+    for name, thr in (("above_atol", ATOL), ("rtol_regime", ATOL / RTOL)):
+        m = np.abs(ref) > thr
+        e = np.abs(y - ref)[m] / np.abs(ref)[m]
+        out[name] = {"max": float(e.max()), "p99_99": float(np.quantile(e, 0.9999)),
+                     "median": float(np.median(e)), "frac_gt_1e-3": float((e > 1e-3).mean()),
+                     "entries": int(m.sum())}
+    return out
 
 
 def main():
@@ -209,61 +242,80 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     import radm2b200
-    from radm2b200 import inputs
+    from radm2b200 import inputs, seeding
 
     ncell, seed, wl, night, dt = WORKLOADS[args.workload]
+    learned = args.method == "learned"
     cells = inputs.make_cells(ncell, seed, wl, night, first_cell=rank * ncell)
     prec = radm2b200.PREC_FP32LU if args.precision == "fp32lu" else radm2b200.PREC_FP64
     sched = radm2b200.SCHED_PERSISTENT if args.schedule == "persistent" else radm2b200.SCHED_STATIC
     refine = 1
-    solver = radm2b200.Solver(precision=prec, schedule=sched, refine_sweeps=refine, device=local,
-                              block_threads=args.block_threads, blocks_per_sm=args.blocks_per_sm)
+    atol, rtol = np.full(59, ATOL), np.full(59, RTOL)
     stream = torch.cuda.Stream()
-    solver.set_stream(stream.cuda_stream)
-    atol, rtol = np.ones(59), np.full(59, 1e-3)
+    ld = (ncell + 31) // 32 * 32
 
     def barrier():
         torch.cuda.synchronize()
         if dist:
             dist.barrier()
 
-    # ---- device-resident leg: inputs in HBM, K splits as one CUDA graph
-    solver.set_cells(cells)
-    ld = (ncell + 31) // 32 * 32
-    y0 = torch.empty((59, ld), dtype=torch.float64, device="cuda")
-    solver.update_rconst()
-    solver.get_state_device(y0.data_ptr(), ld)
-    for _ in range(args.warmup):
-        ipar, rpar = radm2b200.default_params()
-        ierr = solver.run_split(1, dt, atol, rtol, rpar, ipar)
-        assert ierr == 1, "warm-up IERR %d" % ierr
-    solver.set_state_device(y0.data_ptr(), ld)
-    solver.set_kernel_timing(True)
-    ipar, rpar = radm2b200.default_params()
-    solver.run_split(args.steps, dt, atol, rtol, rpar, ipar)  # capture + first replay of the K-split graph
-    solver.set_state_device(y0.data_ptr(), ld)
-    solver.kernel_time()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ipar, rpar = radm2b200.default_params()
-    barrier()
-    with ClockSampler(local) as clocks:
-        ev0.record(stream)
-        ierr = solver.run_split(args.steps, dt, atol, rtol, rpar, ipar)
-        ev1.record(stream)
-        barrier()
-    assert ierr == 1, "IERR %d" % ierr
-    el_ms = ev0.elapsed_time(ev1)
-    kms, klaunch = solver.kernel_time()
-    st = solver.stats()  # last split; totals come from IPAR
-    tot = {"n_accepted": int(ipar[13]), "n_rejected": int(ipar[14])}
-    flops = flops_of(tot, args.precision, refine)
-    if dist:
-        t = torch.tensor([el_ms, kms], dtype=torch.float64, device="cuda")
+    def max_over_ranks(*vals):
+        if not dist:
+            return vals
+        t = torch.tensor(vals, dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        el_ms, kms = float(t[0]), float(t[1])
-    value = ncell * world * args.steps / (el_ms * 1e-3)
+        return tuple(float(x) for x in t)
 
-    # ---- end to end through the C ABI with host buffers (pinned)
+    net, train = None, None
+    if learned:
+        t0 = time.perf_counter()
+        net, train = seeding.train_default(device=local)
+        torch.cuda.synchronize()
+        train["seconds"] = time.perf_counter() - t0
+
+    def timed_arm(solver, attach):
+        """W warm-up splits, then K consecutive splits from the initial state as one CUDA
+        graph, timed with CUDA events on the solver's stream."""
+        solver.set_stream(stream.cuda_stream)
+        solver.set_cells(cells)
+        solver.update_rconst()
+        if attach:
+            solver.attach_mlp(net)
+        y0 = torch.empty((59, ld), dtype=torch.float64, device="cuda")
+        solver.get_state_device(y0.data_ptr(), ld)
+        for _ in range(args.warmup):
+            ipar, rpar = radm2b200.default_params()
+            ierr = solver.run_split(1, dt, atol, rtol, rpar, ipar)
+            assert ierr == 1, "warm-up IERR %d" % ierr
+        solver.set_state_device(y0.data_ptr(), ld)
+        solver.set_kernel_timing(True)
+        ipar, rpar = radm2b200.default_params()
+        solver.run_split(args.steps, dt, atol, rtol, rpar, ipar)  # capture + first replay of the K-split graph
+        solver.set_state_device(y0.data_ptr(), ld)
+        solver.kernel_time()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ipar, rpar = radm2b200.default_params()
+        barrier()
+        with ClockSampler(local) as clocks:
+            ev0.record(stream)
+            ierr = solver.run_split(args.steps, dt, atol, rtol, rpar, ipar)
+            ev1.record(stream)
+            barrier()
+        assert ierr == 1, "IERR %d" % ierr
+        el_ms = ev0.elapsed_time(ev1)
+        kms, klaunch = solver.kernel_time()
+        el_ms, kms = max_over_ranks(el_ms, kms)
+        return {"el_ms": el_ms, "kms": kms, "klaunch": klaunch, "acc": int(ipar[13]), "rej": int(ipar[14]),
+                "clocks": clocks.summary(), "y0": y0}
+
+    # ---- headline arm: inputs resident in HBM, K splits as one CUDA graph
+    solver = radm2b200.Solver(precision=prec, schedule=sched, refine_sweeps=refine, device=local,
+                              block_threads=args.block_threads, blocks_per_sm=args.blocks_per_sm)
+    main_arm = timed_arm(solver, learned)
+    value = ncell * world * args.steps / (main_arm["el_ms"] * 1e-3)
+    y_main = solver.get_state() if rank == 0 else None
+
+    # ---- end to end through the C ABI with host buffers (pinned), same method
     e2e = None
     if not args.no_e2e:
         pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
@@ -286,23 +338,67 @@ def main():
             assert ierr == 1
             cur = hout
         barrier()
-        e2e_s = time.perf_counter() - t0
-        if dist:
-            t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t[0])
+        (e2e_s,) = max_over_ranks(time.perf_counter() - t0)
         e2e = {"value": ncell * world * args.steps / e2e_s, "unit": "cell-steps/s",
                "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo,
-               "path": "radm2_set_inputs + radm2_run_split + radm2_get_state, pinned host AoS buffers"}
+               "path": "radm2_set_inputs + radm2_run_split (%s) + radm2_get_state, pinned host AoS buffers"
+                       % ("network attached: seeding inside the split graph" if learned else "plain")}
+    solver.close()
+
+    # ---- plain FP64 GPU solver on the same K splits (static cell-per-thread, default Hstart)
+    plain = None
+    if learned and not args.no_plain:
+        ps = radm2b200.Solver(precision=radm2b200.PREC_FP64, schedule=radm2b200.SCHED_STATIC, device=local)
+        parm = timed_arm(ps, False)
+        y_plain = ps.get_state() if rank == 0 else None
+        ps.close()
+        pv = ncell * world * args.steps / (parm["el_ms"] * 1e-3)
+        plain = {"value": pv, "ms_per_step": parm["el_ms"] / args.steps, "kernel_ms": parm["kms"],
+                 "method": "FP64, static cell-per-thread schedule, default Hstart 0.01*dt, same graph",
+                 "accepted": parm["acc"], "rejected": parm["rej"], "clocks": parm["clocks"],
+                 "speedup_learned_vs_plain": value / pv}
 
     if rank != 0:
         if dist:
             dist.destroy_process_group()
         return
+
+    # ---- accuracy against an FP64 rtol 1e-8 reference on a subset of cells
+    accuracy = None
+    if args.accuracy_cells > 0:
+        na = min(args.accuracy_cells, ncell)
+        idx = np.linspace(0, ncell - 1, na).astype(np.int64)
+        sub = {k: np.ascontiguousarray(v[idx]) for k, v in cells.items()}
+        with radm2b200.Solver(precision=radm2b200.PREC_FP64, schedule=radm2b200.SCHED_PERSISTENT,
+                              device=local) as ts:
+            ts.set_cells(sub)
+            ipar, rpar = radm2b200.default_params()
+            t0 = time.perf_counter()
+            ierr = ts.run_split(args.steps, dt, atol, np.full(59, RTOL_TIGHT), rpar, ipar, use_graph=False)
+            tight_s = time.perf_counter() - t0
+            assert ierr == 1, "tight reference IERR %d" % ierr
+            y_tight = ts.get_state()
+        # the GPU tight reference checked against the CPU oracle on a few cells
+        nchk = 32
+        y_orc, _ = oracle_sample(sub, nchk, args.steps, dt, RTOL_TIGHT, os.cpu_count() or 1)
+        m = np.abs(y_orc) > 1e-30
+        chk = float((np.abs(y_tight[:nchk] - y_orc)[m] / np.abs(y_orc)[m]).max())
+        accuracy = {"reference": "FP64 rtol 1e-8 (GPU plain path; %d of its cells re-run by the CPU oracle: "
+                                 "max rel diff %.1e)" % (nchk, chk),
+                    "cells": na, "tight_seconds": tight_s,
+                    args.method: rel_errors(y_main[idx], y_tight)}
+        if plain is not None:
+            accuracy["plain"] = rel_errors(y_plain[idx], y_tight)
+            a, b = accuracy[args.method]["above_atol"], accuracy["plain"]["above_atol"]
+            accuracy["learned_no_worse_than_plain"] = bool(a["max"] <= 1.5 * b["max"] + 1e-3 and
+                                                           a["p99_99"] <= 1.5 * b["p99_99"] + 1e-4)
+
     fp64_peak, fp32_peak = radm2b200.fma_peak(local)
+    kms, klaunch = main_arm["kms"], main_arm["klaunch"]
+    flops = flops_of(main_arm["acc"], main_arm["rej"], args.precision, refine)
     per_launch_flops = flops / max(klaunch, 1)
     achieved = per_launch_flops / (kms / max(klaunch, 1) * 1e-3) * 1e-12 if kms > 0 else None
-    traffic = None
+    traffic, traffic_gbs = None, None
     tfile = os.path.join(ROOT, "profiles", "solver_dram_traffic.json")
     if os.path.exists(tfile):
         with open(tfile) as f:
@@ -311,31 +407,51 @@ def main():
         if key in tr:
             # DRAM bytes per step attempt from one ncu capture (small case), scaled to the
             # attempts of an average launch here: traffic grows with attempts, not cells
-            att = (tot["n_accepted"] + tot["n_rejected"]) / max(klaunch, 1)
+            att = (main_arm["acc"] + main_arm["rej"]) / max(klaunch, 1)
             traffic = tr[key]["dram_bytes_per_attempt"] * att
+            if kms > 0:
+                traffic_gbs = traffic / (kms / max(klaunch, 1) * 1e-3) / 1e9
+    peaks = {}
+    pfile = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pfile):
+        with open(pfile) as f:
+            peaks = json.load(f)
+    hbm = peaks.get("hbm_gbs")
+    method = ("learned step seeding (network in the split graph) + persistent work stealing"
+              if learned else "plain") + (", FP32 Jacobian/LU + FP64 refinement" if prec else ", FP64")
     line = {
         "metric": "chem cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": el_ms / args.steps,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": main_arm["el_ms"] / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if args.precision == "fp64" else "f32-LU/f64",
         "data": "synthetic (seeded per-cell distributions; reference WRF inputs not shipped)",
-        "config": {"workload": args.workload, "cells_per_gpu": ncell, "split_s": dt,
-                   "method": "ROS-3, rtol 1e-3, atol 1 molec/cm^3, Hstart 0.01*dt",
+        "config": {"workload": args.workload, "cells_per_gpu": ncell, "seed": seed, "split_s": dt,
+                   "method": method, "tolerances": "rtol 1e-3, atol 1 molec/cm^3, Hstart 0.01*dt",
                    "precision": args.precision, "schedule": args.schedule,
                    "parallelism": "cells sharded over %d GPU(s), no collective" % world,
                    "l2": "inputs (%.1f GB per GPU) larger than L2" % (ncell * 91 * 8 / 1e9),
                    "steps_are": "consecutive 600 s operator splits (K=6 is one simulated hour)"},
-        "gpu_launches": 3 * args.steps,
+        "gpu_launches": (LAUNCHES_PLAIN + (LAUNCHES_SEED if learned else 0)) * args.steps,
         "roofline": {"bound": "fp64" if args.precision == "fp64" else "fp64+fp32", "achieved": achieved,
                      "peak": fp64_peak, "unit": "TFLOP/s",
                      "frac": (achieved / fp64_peak) if achieved else None, "traffic": traffic,
-                     "peak_source": "measured CUDA-core FMA microbenchmark (radm2_fma_peak), FP32 %.1f" % fp32_peak,
-                     "kernel_ms_per_launch": kms / max(klaunch, 1), "flops_per_launch": per_launch_flops},
-        "steps_per_cell": {"accepted": tot["n_accepted"] / ncell / args.steps,
-                           "rejected": tot["n_rejected"] / ncell / args.steps},
-        "clocks": clocks.summary(),
+                     "peak_source": "measured CUDA-core FP64 FMA microbenchmark (radm2_fma_peak); FP32 %.1f"
+                                    % fp32_peak,
+                     "kernel": "k_rosenbrock (solver)",
+                     "kernel_ms_per_launch": kms / max(klaunch, 1), "flops_per_launch": per_launch_flops,
+                     "traffic_gbs": traffic_gbs,
+                     "traffic_frac_of_hbm": (traffic_gbs / hbm) if (traffic_gbs and hbm) else None},
+        "steps_per_cell": {"accepted": main_arm["acc"] / ncell / args.steps,
+                           "rejected": main_arm["rej"] / ncell / args.steps},
+        "clocks": main_arm["clocks"],
         "e2e": e2e,
     }
+    if train is not None:
+        line["training"] = train
+    if plain is not None:
+        line["plain"] = plain
+    if accuracy is not None:
+        line["accuracy"] = accuracy
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cells, dt)
     print(json.dumps(line), flush=True)

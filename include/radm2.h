@@ -222,6 +222,10 @@ int radm2_get_features(radm2_ctx *ctx, double dt, float *out);
 /* Seed the context from the network: per-cell starting steps (set_h0) and the
  * descending-predicted-cost cell order of the persistent schedule (set_order). */
 int radm2_seed_cells(radm2_ctx *ctx, radm2_mlp *mlp, double dt, int set_h0, int set_order);
+/* Attach a network to the context (NULL detaches): every following integration --
+ * radm2_rosenbrock and each split of radm2_run_split -- is seeded from the current
+ * state on the device first, inside the same CUDA graph for radm2_run_split. */
+int radm2_attach_mlp(radm2_ctx *ctx, radm2_mlp *mlp, int set_order);
 
 /* Host-only consistency check of the library's kernel layouts (every thread's
  * working-set offsets inside its allocation, for every built variant). */

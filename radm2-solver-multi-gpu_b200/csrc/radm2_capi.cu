@@ -2,6 +2,7 @@
 // IPAR/RPAR parsing with the reference's checks, kernel launches and the
 // CUDA-graph operator-split loop.
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -308,6 +309,7 @@ cudaError_t launch_solver(radm2_ctx *c, const SolveArgs &a, int bs, int grid)
 // Enqueue one integration of every cell: queue reset, solver, outcome reduction into d_res[slot].
 int enqueue_integration(radm2_ctx *c, const SolveParams &p, int slot, int bs, int grid)
 {
+    if (c->mlp) CK(mlp_enqueue_seed(c, c->mlp, std::fabs(p.Tend - p.Tstart), c->mlp_order));
     CK(cudaMemsetAsync(c->queue + slot, 0, sizeof(int), c->st));
     SolveArgs a = make_args(c, p, c->queue + slot);
     if (c->timing) {
@@ -458,6 +460,9 @@ int radm2_destroy(radm2_ctx *c)
     cudaFree(c->seed_keys);
     cudaFree(c->seed_idx);
     cudaFree(c->seed_tmp);
+    cudaFree(c->seed_x);
+    cudaFree(c->seed_y);
+    if (c->mlp) radm2::mlp_detach(c->mlp);
     if (c->scratch) cudaFree(c->scratch);
     if (c->stage) cudaFree(c->stage);
     if (c->partials) cudaFree(c->partials);
@@ -619,6 +624,7 @@ int radm2_rosenbrock(radm2_ctx *c, double Tstart, double Tend, const double *Abs
     size_t sbytes;
     if ((rc = launch_geometry(c, &bs, &grid, &sbytes))) return rc;
     if ((rc = ensure_scratch(c, sbytes))) return rc;
+    if (c->mlp && (rc = mlp_prepare_seed(c, c->mlp, c->mlp_order))) return rc;
     if ((rc = enqueue_integration(c, p, 0, bs, grid))) return rc;
     CK(cudaMemcpyAsync(c->h_res, c->d_res, sizeof(RunResult), cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
@@ -645,16 +651,25 @@ int radm2_run_split(radm2_ctx *c, int nsplit, double dt, const double *AbsTol, c
     if ((rc = launch_geometry(c, &bs, &grid, &sbytes))) return rc;
     if ((rc = ensure_scratch(c, sbytes))) return rc;
     if ((rc = ensure_results(c, nsplit))) return rc;
+    if (c->mlp && (rc = mlp_prepare_seed(c, c->mlp, c->mlp_order))) return rc;
     if (!use_graph) {
         for (int s = 0; s < nsplit; s++)
             if ((rc = enqueue_integration(c, p, s, bs, grid))) return rc;
         CK(cudaMemcpyAsync(c->h_res, c->d_res, sizeof(RunResult) * nsplit, cudaMemcpyDeviceToHost, c->st));
     } else {
         // The graph bakes in the launch arguments; rebuild it when any of them change.
-        std::vector<unsigned char> key(sizeof(SolveArgs) + 4 * sizeof(int));
         SolveArgs a0 = make_args(c, p, c->queue);
+        const uintptr_t extra[9] = {(uintptr_t)nsplit,
+                                    (uintptr_t)bs,
+                                    (uintptr_t)grid,
+                                    (uintptr_t)(c->o.precision * 4096 + c->o.schedule * 2048 + key_of(c, bs)),
+                                    reinterpret_cast<uintptr_t>(c->mlp),
+                                    (uintptr_t)mlp_generation(c->mlp),
+                                    (uintptr_t)c->mlp_order,
+                                    reinterpret_cast<uintptr_t>(c->seed_x),
+                                    reinterpret_cast<uintptr_t>(c->seed_keys)};
+        std::vector<unsigned char> key(sizeof a0 + sizeof extra);
         std::memcpy(key.data(), &a0, sizeof a0);
-        int extra[4] = {nsplit, bs, grid, (int)(c->o.precision * 4096 + c->o.schedule * 2048 + key_of(c, bs))};
         std::memcpy(key.data() + sizeof a0, extra, sizeof extra);
         if (!c->gexec || key != c->gkey) {
             drop_graph(c);

@@ -455,6 +455,8 @@ struct radm2_mlp {
     int step = 0;
     int nsm = 148;
     float h0_scale = 1.0f;  // seeded h0 = h0_scale * predicted step
+    unsigned int gen = 0;   // bumped when a value that seeding passes by value changes
+    int attached = 0;       // contexts that seed every integration from this network
 };
 
 namespace {
@@ -494,21 +496,27 @@ cudaError_t pack(radm2_mlp *m)
     return cudaGetLastError();
 }
 
-cudaError_t forward(radm2_mlp *m, int n, const float *dx, float *dy, bool keep)
+// Opt the network kernels into their dynamic shared memory, once per process (first
+// call is made outside any stream capture by every entry point that launches them).
+cudaError_t set_kernel_attributes()
 {
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(k_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-        if (e != cudaSuccess) return e;
-        e = cudaFuncSetAttribute(k_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    static bool done = false;
+    if (done) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(k_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    done = e == cudaSuccess;
+    return e;
+}
+
+cudaError_t forward(radm2_mlp *m, int n, const float *dx, float *dy, bool keep, cudaStream_t st)
+{
+    cudaError_t e0 = set_kernel_attributes();
+    if (e0 != cudaSuccess) return e0;
     const size_t zs = (size_t)m->zcap * W;
     const int ntiles = (n + ROWS - 1) / ROWS;
     const int grid = ntiles < m->nsm ? ntiles : m->nsm;  // one CTA per SM walks the row tiles
     (void)cudaGetLastError();
-    k_forward<<<grid, 128, SMEM_BYTES, m->st>>>(net_of(m), n, dx, dy, keep ? m->z : nullptr,
+    k_forward<<<grid, 128, SMEM_BYTES, st>>>(net_of(m), n, dx, dy, keep ? m->z : nullptr,
                                                                  keep ? m->z + zs : nullptr,
                                                                  keep ? m->z + 2 * zs : nullptr);
     return cudaGetLastError();
@@ -525,6 +533,69 @@ cudaError_t backward(radm2_mlp *m, int n, const float *dx, const float *dt)
 }
 
 }  // namespace
+
+// Allocate what seeding a context needs (h0, feature and prediction rows, sort keys, and
+// the order with its sort workspace when asked).  The rows belong to the context, so a
+// captured graph never reads buffers that the network may reallocate; nothing is
+// allocated again while the cell count stays the same.
+int radm2::mlp_prepare_seed(radm2_ctx *c, radm2_mlp *m, bool order)
+{
+    (void)m;
+    const int n = c->ncell;
+    cudaError_t e = set_kernel_attributes();
+    if (e == cudaSuccess && !c->h0) e = cudaMalloc((void **)&c->h0, sizeof(double) * c->ld);
+    if (e == cudaSuccess && order && !c->order) e = cudaMalloc((void **)&c->order, sizeof(int) * c->ld);
+    if (e == cudaSuccess && c->seed_cap < n) {
+        void *old[] = {c->seed_keys, c->seed_idx, c->seed_tmp, c->seed_x, c->seed_y};
+        for (void *q : old) cudaFree(q);
+        c->seed_keys = nullptr;
+        c->seed_idx = nullptr;
+        c->seed_tmp = nullptr;
+        c->seed_x = c->seed_y = nullptr;
+        c->seed_tmp_bytes = 0;
+        c->seed_cap = 0;
+        e = cudaMalloc((void **)&c->seed_keys, sizeof(unsigned int) * (size_t)n * 2);
+        if (e == cudaSuccess) e = cudaMalloc((void **)&c->seed_idx, sizeof(int) * (size_t)n);
+        if (e == cudaSuccess) e = cudaMalloc((void **)&c->seed_x, sizeof(float) * (size_t)n * NFEAT);
+        if (e == cudaSuccess) e = cudaMalloc((void **)&c->seed_y, sizeof(float) * (size_t)n * NY);
+        if (e == cudaSuccess) c->seed_cap = n;
+    }
+    if (e == cudaSuccess && order && !c->seed_tmp) {
+        e = cub::DeviceRadixSort::SortPairs(nullptr, c->seed_tmp_bytes, c->seed_keys, c->seed_keys + n, c->seed_idx,
+                                            c->order, n, 0, 32, c->st);
+        if (e == cudaSuccess) e = cudaMalloc(&c->seed_tmp, c->seed_tmp_bytes);
+    }
+    if (e != cudaSuccess) {
+        c->err = std::string("seeding buffers: ") + cudaGetErrorString(e);
+        return RADM2_E_NOMEM;
+    }
+    return RADM2_OK;
+}
+
+unsigned int radm2::mlp_generation(const radm2_mlp *m) { return m ? m->gen : 0u; }
+void radm2::mlp_detach(radm2_mlp *m) { m->attached--; }
+
+// Stream-ordered seeding on the context's stream (capturable): features -> network ->
+// per-cell h0 (and the descending-cost order when asked).
+cudaError_t radm2::mlp_enqueue_seed(radm2_ctx *c, radm2_mlp *m, double dt, bool order)
+{
+    const int n = c->ncell;
+    (void)cudaGetLastError();
+    k_features<<<(n + 127) / 128, 128, 0, c->st>>>(n, c->ld, c->var, c->fix, c->temp, c->jv, (float)dt, c->seed_x);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = forward(m, n, c->seed_x, c->seed_y, false, c->st);
+    if (e == cudaSuccess) {
+        k_seed<<<(n + 127) / 128, 128, 0, c->st>>>(n, c->seed_y, m->ymean[0], m->ystd[0], m->ymean[1], m->ystd[1],
+                                                   m->h0_scale, c->h0, c->seed_keys, c->seed_idx);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && order) {
+        size_t tb = c->seed_tmp_bytes;
+        e = cub::DeviceRadixSort::SortPairs(c->seed_tmp, tb, c->seed_keys, c->seed_keys + n, c->seed_idx, c->order, n,
+                                            0, 32, c->st);
+    }
+    return e;
+}
 
 extern "C" {
 
@@ -586,6 +657,7 @@ int radm2_mlp_create(radm2_mlp **out, int device, unsigned int seed)
 int radm2_mlp_destroy(radm2_mlp *m)
 {
     if (!m) return RADM2_E_ARG;
+    if (m->attached > 0) return RADM2_E_STATE;  // still attached to a context
     cudaSetDevice(m->device);
     if (m->st) cudaStreamSynchronize(m->st);
     void *ptrs[] = {m->p, m->g, m->m, m->v, m->wt, m->xmean, m->xstd, m->loss, m->z, m->y, m->xbuf, m->tbuf};
@@ -628,6 +700,7 @@ int radm2_mlp_set_norm(radm2_mlp *m, const float *xmean, const float *xstd, cons
         m->ymean[k] = ymean[k];
         m->ystd[k] = ystd[k] > 0.f ? ystd[k] : 1.f;
     }
+    m->gen++;
     cudaSetDevice(m->device);
     if (cudaMemcpy(m->xmean, mm, sizeof mm, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(m->xstd, ss, sizeof ss, cudaMemcpyHostToDevice) != cudaSuccess)
@@ -642,7 +715,7 @@ int radm2_mlp_forward(radm2_mlp *m, int n, const float *x, float *y)
     int rc = mlp_ensure(m, n, false);
     if (rc) return rc;
     if (cudaMemcpyAsync(m->xbuf, x, sizeof(float) * (size_t)n * NFEAT, cudaMemcpyHostToDevice, m->st) != cudaSuccess ||
-        forward(m, n, m->xbuf, m->y, false) != cudaSuccess ||
+        forward(m, n, m->xbuf, m->y, false, m->st) != cudaSuccess ||
         cudaMemcpyAsync(y, m->y, sizeof(float) * (size_t)n * NY, cudaMemcpyDeviceToHost, m->st) != cudaSuccess ||
         cudaStreamSynchronize(m->st) != cudaSuccess)
         return RADM2_E_CUDA;
@@ -658,7 +731,7 @@ int radm2_mlp_gradients(radm2_mlp *m, int n, const float *x, const float *target
     if (cudaMemcpyAsync(m->xbuf, x, sizeof(float) * (size_t)n * NFEAT, cudaMemcpyHostToDevice, m->st) != cudaSuccess ||
         cudaMemcpyAsync(m->tbuf, target, sizeof(float) * (size_t)n * NY, cudaMemcpyHostToDevice, m->st) != cudaSuccess ||
         cudaMemsetAsync(m->g, 0, sizeof(float) * NPARAM, m->st) != cudaSuccess ||
-        forward(m, n, m->xbuf, m->y, true) != cudaSuccess || backward(m, n, m->xbuf, m->tbuf) != cudaSuccess ||
+        forward(m, n, m->xbuf, m->y, true, m->st) != cudaSuccess || backward(m, n, m->xbuf, m->tbuf) != cudaSuccess ||
         cudaMemcpyAsync(grad, m->g, sizeof(float) * NPARAM, cudaMemcpyDeviceToHost, m->st) != cudaSuccess ||
         cudaMemcpyAsync(loss, m->loss, sizeof(float), cudaMemcpyDeviceToHost, m->st) != cudaSuccess ||
         cudaMemsetAsync(m->g, 0, sizeof(float) * NPARAM, m->st) != cudaSuccess ||
@@ -676,7 +749,7 @@ int radm2_mlp_train_step(radm2_mlp *m, int n, const float *dx, const float *dtar
     m->step++;
     const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
     const float c1 = 1.f - powf(b1, (float)m->step), c2 = 1.f - powf(b2, (float)m->step);
-    if (forward(m, n, dx, m->y, true) != cudaSuccess || backward(m, n, dx, dtarget) != cudaSuccess)
+    if (forward(m, n, dx, m->y, true, m->st) != cudaSuccess || backward(m, n, dx, dtarget) != cudaSuccess)
         return RADM2_E_CUDA;
     k_adam<<<(NPARAM + 255) / 256, 256, 0, m->st>>>(NPARAM, m->p, m->g, m->m, m->v, lr, b1, b2, eps, c1, c2);
     if (cudaGetLastError() != cudaSuccess || pack(m) != cudaSuccess) return RADM2_E_CUDA;
@@ -692,6 +765,7 @@ int radm2_mlp_set_h0_scale(radm2_mlp *m, float scale)
 {
     if (!m || !(scale > 0.f)) return RADM2_E_ARG;
     m->h0_scale = scale;
+    m->gen++;
     return RADM2_OK;
 }
 
@@ -722,56 +796,39 @@ int radm2_seed_cells(radm2_ctx *c, radm2_mlp *m, double dt, int set_h0, int set_
     if (!c || !m || !(dt > 0.0)) return RADM2_E_ARG;
     if (!c->var) return RADM2_E_STATE;
     cudaSetDevice(c->o.device);
-    const int n = c->ncell;
-    int rc = mlp_ensure(m, n, false);
+    int rc = radm2::mlp_prepare_seed(c, m, set_order != 0);
     if (rc) return rc;
-    // Work arrays live in the context and are reused across calls (no per-call allocation
-    // once they exist).  A cached split graph reads h0 / order from device memory when it
-    // runs; only their first allocation changes its arguments, which the graph key sees.
-    cudaError_t e = cudaSuccess;
-    if (!c->h0) e = cudaMalloc((void **)&c->h0, sizeof(double) * c->ld);
-    if (e == cudaSuccess && !c->order) e = cudaMalloc((void **)&c->order, sizeof(int) * c->ld);
-    if (e == cudaSuccess && c->seed_cap < n) {
-        cudaFree(c->seed_keys);
-        cudaFree(c->seed_idx);
-        cudaFree(c->seed_tmp);
-        c->seed_keys = nullptr;
-        c->seed_idx = nullptr;
-        c->seed_tmp = nullptr;
-        c->seed_cap = 0;
-        e = cudaMalloc((void **)&c->seed_keys, sizeof(unsigned int) * (size_t)n * 2);
-        if (e == cudaSuccess) e = cudaMalloc((void **)&c->seed_idx, sizeof(int) * (size_t)n);
-        if (e == cudaSuccess) e = cub::DeviceRadixSort::SortPairs(nullptr, c->seed_tmp_bytes, c->seed_keys,
-                                                                  c->seed_keys + n, c->seed_idx, c->order, n, 0, 32,
-                                                                  c->st);
-        if (e == cudaSuccess) e = cudaMalloc(&c->seed_tmp, c->seed_tmp_bytes);
-        if (e == cudaSuccess) c->seed_cap = n;
-    }
-    // the network runs on the context's stream so it orders with the solver
-    cudaStream_t keep = m->st;
-    m->st = c->st;
-    if (e == cudaSuccess) {
-        (void)cudaGetLastError();
-        k_features<<<(n + 127) / 128, 128, 0, c->st>>>(n, c->ld, c->var, c->fix, c->temp, c->jv, (float)dt, m->xbuf);
-        e = cudaGetLastError();
-    }
-    if (e == cudaSuccess) e = forward(m, n, m->xbuf, m->y, false);
-    if (e == cudaSuccess) {
-        k_seed<<<(n + 127) / 128, 128, 0, c->st>>>(n, m->y, m->ymean[0], m->ystd[0], m->ymean[1], m->ystd[1], m->h0_scale, c->h0,
-                                                   c->seed_keys, c->seed_idx);
-        e = cudaGetLastError();
-    }
-    if (e == cudaSuccess && set_order) {
-        size_t tb = c->seed_tmp_bytes;
-        e = cub::DeviceRadixSort::SortPairs(c->seed_tmp, tb, c->seed_keys, c->seed_keys + n, c->seed_idx, c->order, n,
-                                            0, 32, c->st);
-    }
-    m->st = keep;
-    if (e != cudaSuccess) {
-        c->err = std::string("radm2_seed_cells: ") + cudaGetErrorString(e);
+    if (radm2::mlp_enqueue_seed(c, m, dt, set_order != 0) != cudaSuccess || cudaStreamSynchronize(c->st) != cudaSuccess) {
+        c->err = "radm2_seed_cells: CUDA error";
         return RADM2_E_CUDA;
     }
     c->use_h0 = set_h0 != 0;
+    c->use_order = set_order != 0;
+    return RADM2_OK;
+}
+
+int radm2_attach_mlp(radm2_ctx *c, radm2_mlp *m, int set_order)
+{
+    if (!c) return RADM2_E_ARG;
+    if (!c->var) return RADM2_E_STATE;
+    cudaSetDevice(c->o.device);
+    if (m && m->device != c->o.device) {
+        c->err = "radm2_attach_mlp: network and context are on different devices";
+        return RADM2_E_ARG;
+    }
+    if (m) {
+        int rc = radm2::mlp_prepare_seed(c, m, set_order != 0);
+        if (rc) return rc;
+    }
+    radm2::ctx_drop_graph(c);
+    if (c->mlp) c->mlp->attached--;
+    c->mlp = m;
+    c->mlp_order = m && set_order;
+    if (!m) return RADM2_OK;
+    m->attached++;
+    // the network's stream may still be writing its weights (training)
+    if (cudaStreamSynchronize(m->st) != cudaSuccess) return RADM2_E_CUDA;
+    c->use_h0 = true;
     c->use_order = set_order != 0;
     return RADM2_OK;
 }

@@ -17,6 +17,8 @@ NVAR, NFIX, NREACT, NPH, NJVS = 59, 2, 156, 28, 659
 PREC_FP64, PREC_FP32LU = 0, 1
 PLACE_GLOBAL, PLACE_LU_SMEM, PLACE_ALL_SMEM = 0, 1, 3
 SCHED_STATIC, SCHED_PERSISTENT = 0, 1
+RADM2_OK, RADM2_E_ARG, RADM2_E_CUDA, RADM2_E_NOMEM, RADM2_E_STATE, RADM2_E_NODEV, RADM2_E_TOOBIG = \
+    0, -100, -101, -102, -103, -104, -105
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(os.path.dirname(_HERE), "libradm2_b200.so")
@@ -86,6 +88,7 @@ SIGNATURES = {
     "radm2_get_features": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, _F]),
     "radm2_seed_cells": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_int,
                                         ctypes.c_int]),
+    "radm2_attach_mlp": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]),
     "radm2_get_ncell": (ctypes.c_int, [ctypes.c_void_p]),
     "radm2_device_bytes": (ctypes.c_size_t, [ctypes.c_void_p]),
     "radm2_rosenbrock_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
@@ -176,8 +179,9 @@ class Solver:
 
     def close(self):
         if getattr(self, "h", None):
-            self.lib.radm2_destroy(self.h)
+            self.lib.radm2_destroy(self.h)  # detaches an attached network
             self.h = None
+            self._mlp = None
 
     def __del__(self):
         try:
@@ -299,6 +303,11 @@ class Solver:
         self._check(self.lib.radm2_get_features(self.h, dt, out.ctypes.data_as(_F)))
         return out
 
+    def attach_mlp(self, mlp, order=False):
+        """Seed every following integration from the network (None detaches)."""
+        self._check(self.lib.radm2_attach_mlp(self.h, mlp.h if mlp is not None else None, 1 if order else 0))
+        self._mlp = mlp  # keep the network alive while attached
+
     def seed_cells(self, mlp, dt, h0=True, order=True):
         self._check(self.lib.radm2_seed_cells(self.h, mlp.h, dt, 1 if h0 else 0, 1 if order else 0))
 
@@ -338,8 +347,8 @@ class Mlp:
         self.nparams = self.lib.radm2_mlp_nparams()
 
     def close(self):
-        if getattr(self, "h", None):
-            self.lib.radm2_mlp_destroy(self.h)
+        # refused (RADM2_E_STATE) while a context still seeds from this network
+        if getattr(self, "h", None) and self.lib.radm2_mlp_destroy(self.h) == RADM2_OK:
             self.h = None
 
     def __del__(self):

@@ -6,8 +6,9 @@ Labels come from the plain FP64 solver itself: for every cell and operator split
 first accepted step size (the h0 that would have avoided the initial rejections) and the
 number of accepted steps of that split.  At use, the predictions seed per-cell starting
 steps (the Rosenbrock error controller still judges every step; invalid predictions fall
-back to the default Hstart) and order cells by descending predicted cost for the
-persistent schedule.
+back to the default Hstart) and, optionally, order cells by descending predicted cost
+for the persistent schedule.  Attached to a solver (Solver.attach_mlp), the seeding
+kernels run in front of every split inside the split loop's CUDA graph.
 """
 import numpy as np
 
@@ -86,10 +87,28 @@ def fit(X, Y, epochs=6, batch=4096, lr=2e-3, seed=0, device=0, log=None):
     return net, history
 
 
+# The training recipe: traces of 262,144 cells x 8 splits (2.1 M state/label pairs) of the
+# mixed-regime distribution under a seed disjoint from every evaluation batch, labels from
+# splits started at h0 = dt, 6 epochs; seeded steps are half the predicted step.
+TRAIN_CELLS, TRAIN_SPLITS, TRAIN_SEED, TRAIN_EPOCHS, H0_SAFETY = 262144, 8, 100, 6, 0.5
+
+
+def train_default(device=0, dt=600.0, log=None):
+    """Generate traces with the solver and train the seeding network on the GPU.
+    Returns (net, info) with the pair count and the final training loss."""
+    X, Y = generate_traces(TRAIN_CELLS, TRAIN_SPLITS, TRAIN_SEED, dt=dt, workload="mixed")
+    net, hist = fit(X, Y, epochs=TRAIN_EPOCHS, seed=0, device=device, log=log)
+    net.set_h0_scale(H0_SAFETY)
+    return net, {"pairs": int(X.shape[0]), "loss": float(hist[-1]), "epochs": TRAIN_EPOCHS,
+                 "trace_cells": TRAIN_CELLS, "trace_splits": TRAIN_SPLITS, "trace_seed": TRAIN_SEED,
+                 "h0_safety": H0_SAFETY}
+
+
 def evaluate_split_loop(cells, nsplit, dt=600.0, net=None, precision=PREC_FP64, schedule=SCHED_PERSISTENT,
-                        use_h0=True, use_order=True, timer=None, safety=None, carry=False):
+                        use_h0=True, use_order=True, timer=None, safety=None, carry=False, attach=False):
     """Integrate nsplit consecutive splits; with a network, seed every split from it
-    (h0 = safety * predicted step); with carry, start each split from the step size the
+    (h0 = safety * predicted step) -- host-driven per split, or with attach=True inside one
+    CUDA graph of all nsplit splits; with carry, start each split from the step size the
     previous split ended with.  Returns (final state, totals, seconds, solver-kernel ms)."""
     tot = {"acc": 0, "rej": 0}
     with Solver(precision=precision, schedule=schedule) as s:
@@ -99,6 +118,21 @@ def evaluate_split_loop(cells, nsplit, dt=600.0, net=None, precision=PREC_FP64, 
         s.synchronize()
         if net is not None and safety is not None:
             net.set_h0_scale(safety)
+        if attach and net is not None:
+            s.attach_mlp(net, order=use_order and schedule == SCHED_PERSISTENT)
+            ipar, rpar = default_params()
+            t0 = timer() if timer else None
+            ierr = s.run_split(nsplit, dt, ATOL, RTOL, rpar, ipar, use_graph=True)
+            if ierr != 1:
+                raise RuntimeError("IERR %d" % ierr)
+            tot["acc"] += int(ipar[13])
+            tot["rej"] += int(ipar[14])
+            s.synchronize()
+            el = (timer() - t0) if timer else None
+            kms, _ = s.kernel_time()
+            y = s.get_state()
+            s.attach_mlp(None)
+            return y, tot, el, kms
         t0 = timer() if timer else None
         for k in range(nsplit):
             if net is not None:

@@ -43,3 +43,11 @@ def test_kernel_layouts_in_bounds():
     """Every built solver variant's per-thread working-set offsets fit its allocation
     (host-side arithmetic over the same layout constants the kernels use)."""
     assert radm2b200.load().radm2_selfcheck() == 0
+
+
+def test_error_codes_match_header():
+    text = open(os.path.join(ROOT, "include", "radm2.h")).read()
+    codes = {m.group(1): int(m.group(2)) for m in re.finditer(r"#define (RADM2_(?:OK|E_\w+))\s+\(?(-?\d+)\)?", text)}
+    assert len(codes) == 7
+    for name, val in codes.items():
+        assert getattr(rlib, name) == val, name

@@ -88,3 +88,34 @@ def test_training_reduces_loss_and_gains_steps():
     e1 = (np.abs(y1[idx] - yt)[above] / np.abs(yt)[above]).max()
     print("max rel err vs rtol-1e-8 oracle: default %.2e learned %.2e" % (e0, e1))
     assert e1 <= 1.5 * e0 + 1e-3
+
+
+def test_attached_seeding_in_graph_matches_host_driven():
+    """A network attached to the context seeds every split inside the split loop's CUDA
+    graph; the result is bit-identical to seeding each split from the host."""
+    cells = inputs.make_cells(4096, 12, "mixed")
+    with radm2b200.Solver() as s:
+        s.set_cells(cells)
+        x = s.features(600.0)
+    net, _, _ = _net(x, seed=5)
+    net.set_norm(x.mean(0), np.where(x.std(0) > 1e-6, x.std(0), 1.0), np.array([0.5, 0.7]), np.array([0.6, 0.3]))
+    net.set_h0_scale(0.5)
+    y_host, t_host, _, _ = seeding.evaluate_split_loop(cells, 3, net=net, use_order=False)
+    y_att, t_att, _, _ = seeding.evaluate_split_loop(cells, 3, net=net, use_order=False, attach=True)
+    assert t_host == t_att
+    assert np.array_equal(y_host, y_att)
+    # the graph is rebuilt when a value baked into it changes (the h0 scale)
+    with radm2b200.Solver() as s:
+        s.set_cells(cells)
+        s.attach_mlp(net)
+        ipar, rpar = radm2b200.default_params()
+        assert s.run_split(2, 600.0, seeding.ATOL, seeding.RTOL, rpar, ipar) == 1
+        acc_a = int(ipar[13])
+        s.set_cells(cells)
+        net.set_h0_scale(0.05)
+        ipar, rpar = radm2b200.default_params()
+        assert s.run_split(2, 600.0, seeding.ATOL, seeding.RTOL, rpar, ipar) == 1
+        assert int(ipar[13]) != acc_a
+        # a network still attached cannot be destroyed
+        assert radm2b200.lib.load().radm2_mlp_destroy(net.h) == radm2b200.lib.RADM2_E_STATE
+        s.attach_mlp(None)
