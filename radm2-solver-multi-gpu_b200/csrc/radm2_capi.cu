@@ -306,6 +306,18 @@ cudaError_t launch_solver(radm2_ctx *c, const SolveArgs &a, int bs, int grid)
     return pers ? launch_solver_fp64_persistent(a, k, grid, c->st) : launch_solver_fp64_static(a, k, grid, c->st);
 }
 
+// Record a kernel-timing event.  Under stream capture the External flag makes the record
+// a graph node (re-recorded on every replay); outside capture it is a plain record (the
+// flag is only valid while capturing).
+cudaError_t record_timing_event(radm2_ctx *c, cudaEvent_t ev)
+{
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(c->st, &cs);
+    if (e != cudaSuccess) return e;
+    return cs == cudaStreamCaptureStatusActive ? cudaEventRecordWithFlags(ev, c->st, cudaEventRecordExternal)
+                                               : cudaEventRecord(ev, c->st);
+}
+
 // Enqueue one integration of every cell: queue reset, solver, outcome reduction into d_res[slot].
 int enqueue_integration(radm2_ctx *c, const SolveParams &p, int slot, int bs, int grid)
 {
@@ -318,12 +330,11 @@ int enqueue_integration(radm2_ctx *c, const SolveParams &p, int slot, int bs, in
             CK(cudaEventCreate(&e));
             c->ev.push_back(e);
         }
-        // External flag: under stream capture the record becomes a graph node (re-recorded per replay).
-        CK(cudaEventRecordWithFlags(c->ev[2 * slot], c->st, cudaEventRecordExternal));
+        CK(record_timing_event(c, c->ev[2 * slot]));
     }
     CK(launch_solver(c, a, bs, grid));
     if (c->timing) {
-        CK(cudaEventRecordWithFlags(c->ev[2 * slot + 1], c->st, cudaEventRecordExternal));
+        CK(record_timing_event(c, c->ev[2 * slot + 1]));
         if (slot + 1 > c->ev_used) c->ev_used = slot + 1;
     }
     CK(launch_reduce(c->ncell, c->status, c->nacc, c->nrej, c->texit, c->hexit, c->partials, c->d_res + slot, c->st));
@@ -662,7 +673,8 @@ int radm2_run_split(radm2_ctx *c, int nsplit, double dt, const double *AbsTol, c
         const uintptr_t extra[9] = {(uintptr_t)nsplit,
                                     (uintptr_t)bs,
                                     (uintptr_t)grid,
-                                    (uintptr_t)(c->o.precision * 4096 + c->o.schedule * 2048 + key_of(c, bs)),
+                                    (uintptr_t)((c->o.precision * 2 + c->o.schedule) * (1ull << 32) +
+                                                (unsigned)key_of(c, bs)),
                                     reinterpret_cast<uintptr_t>(c->mlp),
                                     (uintptr_t)mlp_generation(c->mlp),
                                     (uintptr_t)c->mlp_order,

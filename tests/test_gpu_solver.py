@@ -193,3 +193,17 @@ def test_fp32_lu_accuracy(cells4k):
     e32 = np.abs(y32 - y_tight)[above] / np.abs(y_tight)[above]
     e64 = np.abs(y64 - y_tight)[above] / np.abs(y_tight)[above]
     assert e32.max() <= e64.max() * 1.01 + 1e-9
+
+
+def test_kernel_timing_with_and_without_graph():
+    """Solver-kernel timing works for host-driven splits and inside the split graph."""
+    cells = inputs.make_cells(2048, 4, "plain", 0.3)
+    for use_graph in (False, True):
+        with radm2b200.Solver(schedule=radm2b200.SCHED_PERSISTENT) as s:
+            s.set_cells(cells)
+            s.set_kernel_timing(True)
+            ipar, rpar = radm2b200.default_params()
+            assert s.run_split(2, 600.0, np.ones(59), np.full(59, 1e-3), rpar, ipar, use_graph=use_graph) == 1
+            ms, n = s.kernel_time()
+            assert n == 2 and ms > 0.0, (use_graph, ms, n)
+
