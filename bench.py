@@ -69,9 +69,12 @@ def parse():
     ap.add_argument("--method", default="learned", choices=["learned", "plain"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32lu"])
     ap.add_argument("--schedule", default="persistent", choices=["static", "persistent"])
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shape")
     ap.add_argument("--block-threads", type=int, default=0)
     ap.add_argument("--blocks-per-sm", type=int, default=0)
     ap.add_argument("--accuracy-cells", type=int, default=8192)
+    ap.add_argument("--weights", default="", help="seeding network stored by --save-weights (skip training)")
+    ap.add_argument("--save-weights", default="")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain comparison arm")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -267,18 +270,32 @@ def main():
         return tuple(float(x) for x in t)
 
     net, train = None, None
-    if learned:
+    if learned and args.weights:
+        net = seeding.load_net(args.weights, device=local)
+        train = {"loaded": os.path.basename(args.weights)}
+    elif learned:
         t0 = time.perf_counter()
         net, train = seeding.train_default(device=local)
         torch.cuda.synchronize()
         train["seconds"] = time.perf_counter() - t0
+        if args.save_weights and rank == 0:
+            seeding.save_net(net, args.save_weights)
 
-    def timed_arm(solver, attach):
-        """W warm-up splits, then K consecutive splits from the initial state as one CUDA
-        graph, timed with CUDA events on the solver's stream."""
+    def timed_arm(solver, attach, tune=False):
+        """(Autotune,) W warm-up splits, then K consecutive splits from the initial state as
+        one CUDA graph, timed with CUDA events on the solver's stream."""
         solver.set_stream(stream.cuda_stream)
         solver.set_cells(cells)
         solver.update_rconst()
+        tuned = None
+        if tune:
+            t0 = time.perf_counter()
+            table = solver.autotune(dt, atol, rtol)
+            o = solver.opts()
+            tuned = {"chosen": {k: o[k] for k in ("schedule", "block_threads", "placement", "min_blocks")},
+                     "seconds": time.perf_counter() - t0, "sample_cells": min(ncell, 262144),
+                     "candidates": [[t["schedule"], t["block_threads"], t["placement"], t["min_blocks"],
+                                     round(t["ms"], 2)] for t in table]}
         if attach:
             solver.attach_mlp(net)
         y0 = torch.empty((59, ld), dtype=torch.float64, device="cuda")
@@ -306,12 +323,13 @@ def main():
         kms, klaunch = solver.kernel_time()
         el_ms, kms = max_over_ranks(el_ms, kms)
         return {"el_ms": el_ms, "kms": kms, "klaunch": klaunch, "acc": int(ipar[13]), "rej": int(ipar[14]),
-                "clocks": clocks.summary(), "y0": y0}
+                "clocks": clocks.summary(), "y0": y0, "tuned": tuned}
 
     # ---- headline arm: inputs resident in HBM, K splits as one CUDA graph
     solver = radm2b200.Solver(precision=prec, schedule=sched, refine_sweeps=refine, device=local,
                               block_threads=args.block_threads, blocks_per_sm=args.blocks_per_sm)
-    main_arm = timed_arm(solver, learned)
+    tune = not args.no_autotune and not args.block_threads and not args.blocks_per_sm
+    main_arm = timed_arm(solver, learned, tune=tune)
     value = ncell * world * args.steps / (main_arm["el_ms"] * 1e-3)
     y_main = solver.get_state() if rank == 0 else None
 
@@ -403,7 +421,10 @@ def main():
     if os.path.exists(tfile):
         with open(tfile) as f:
             tr = json.load(f)
-        key = "%s-%s" % (args.precision, args.schedule)
+        sched_used = args.schedule
+        if main_arm["tuned"] is not None:
+            sched_used = "persistent" if main_arm["tuned"]["chosen"]["schedule"] else "static"
+        key = "%s-%s" % (args.precision, sched_used)
         if key in tr:
             # DRAM bytes per step attempt from one ncu capture (small case), scaled to the
             # attempts of an average launch here: traffic grows with attempts, not cells
@@ -446,6 +467,12 @@ def main():
         "clocks": main_arm["clocks"],
         "e2e": e2e,
     }
+    if main_arm["tuned"] is not None:
+        line["autotune"] = main_arm["tuned"]
+        ch = main_arm["tuned"]["chosen"]
+        line["config"]["schedule"] = "persistent" if ch["schedule"] else "static"
+        line["config"]["launch"] = "%d threads/block, placement %d, min blocks %d (autotuned)" % (
+            ch["block_threads"], ch["placement"], ch["min_blocks"])
     if train is not None:
         line["training"] = train
     if plain is not None:

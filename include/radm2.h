@@ -187,6 +187,23 @@ int radm2_fma_peak(int device, double *fp64_tflops, double *fp32_tflops);
 
 /* Number of cells and device bytes held by the context. */
 int radm2_get_ncell(const radm2_ctx *ctx);
+int radm2_get_opts(const radm2_ctx *ctx, radm2_opts *out);  /* options in force (after autotune) */
+
+/* Autotuner (no counterpart in the reference, which has one fixed launch shape).  Times
+ * every built solver variant of the context's precision -- static and persistent
+ * schedules x block size x placement of the working set (global scratch / shared memory)
+ * x register cap -- on a strided sample of the context's current cells (sample_cells;
+ * 0 = 262,144) for one split of length dt with the given tolerances and parameters, and
+ * keeps the fastest in the context's options (radm2_get_opts reads them).  The context's
+ * cells and state are not changed.  table (may be NULL) receives up to table_len
+ * entries, n_entries the number of candidates. */
+typedef struct radm2_tune_entry {
+    int schedule, block_threads, placement, min_blocks; /* the candidate */
+    double ms;                                          /* solver-kernel time, -1 = did not run */
+    long long attempts;                                 /* step attempts of the sample split */
+} radm2_tune_entry;
+int radm2_autotune(radm2_ctx *ctx, double dt, const double *AbsTol, const double *RelTol, const double *RPAR,
+                   const int *IPAR, int sample_cells, radm2_tune_entry *table, int table_len, int *n_entries);
 size_t radm2_device_bytes(const radm2_ctx *ctx);
 
 /*

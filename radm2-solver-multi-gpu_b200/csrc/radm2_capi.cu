@@ -1,6 +1,7 @@
 // C ABI of the B200 RADM2 solver (include/radm2.h): context, device buffers,
 // IPAR/RPAR parsing with the reference's checks, kernel launches and the
 // CUDA-graph operator-split loop.
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -795,6 +796,144 @@ int radm2_get_kernel_time(radm2_ctx *c, double *ms, int *launches)
 }
 
 int radm2_get_ncell(const radm2_ctx *c) { return c ? c->ncell : RADM2_E_ARG; }
+
+int radm2_get_opts(const radm2_ctx *c, radm2_opts *out)
+{
+    if (!c || !out) return RADM2_E_ARG;
+    *out = c->o;
+    return RADM2_OK;
+}
+
+// ---------------------------------------------------------------- autotuner
+//
+// Times every built solver variant of the context's precision -- both schedules, every
+// (block size, placement, register cap) -- on a strided sample of the context's own cells
+// for one split, in a scratch context on the same device, and writes the fastest into the
+// context's options.  Every candidate integrates the same sample from the same state and
+// must take the same steps; the solver-kernel time (CUDA events) decides.
+int radm2_autotune(radm2_ctx *c, double dt, const double *AbsTol, const double *RelTol, const double *RPAR,
+                   const int *IPAR, int sample_cells, radm2_tune_entry *table, int table_len, int *n_entries)
+{
+    if (!valid_ctx(c) || !(dt > 0.0) || !AbsTol || !RelTol || !RPAR || !IPAR || sample_cells < 0 || table_len < 0 ||
+        (table_len > 0 && !table))
+        return RADM2_E_ARG;
+    if (!c->var) return RADM2_E_STATE;
+    CK(cudaSetDevice(c->o.device));
+    const int n = std::min(c->ncell, sample_cells > 0 ? sample_cells : 262144);
+    const int stride = c->ncell / n;
+
+    struct Cand {
+        int sched, bs, place, minb;
+    };
+    std::vector<Cand> cands;
+    for (int sched = RADM2_SCHED_STATIC; sched <= RADM2_SCHED_PERSISTENT; sched++) {
+#define RADM2_TUNE_CAND(BS_, PL_, MB_) cands.push_back({sched, BS_, PL_, MB_});
+        if (c->o.precision == RADM2_PREC_FP32LU) {
+            RADM2_VARIANTS_FP32(RADM2_TUNE_CAND)
+        } else {
+            RADM2_VARIANTS_FP64(RADM2_TUNE_CAND)
+        }
+#undef RADM2_TUNE_CAND
+    }
+
+    // scratch context holding the strided sample (its own stream; the caller's stream is
+    // drained first so the sample sees the current state)
+    CK(cudaStreamSynchronize(c->st));
+    radm2_ctx *t = nullptr;
+    int rc = radm2_create(&t, &c->o);
+    if (rc) return rc;
+    double *y0 = nullptr;
+    auto fail = [&](int code) {
+        if (y0) cudaFree(y0);
+        radm2_destroy(t);
+        return code;
+    };
+    if ((rc = ensure_cells(t, n))) {
+        c->err = t->err;
+        return fail(rc);
+    }
+    cudaError_t e = launch_gather_rows(n, NVAR, c->ld, stride, c->var, t->ld, t->var, t->st);
+    if (e == cudaSuccess) e = launch_gather_rows(n, NFIX, c->ld, stride, c->fix, t->ld, t->fix, t->st);
+    if (e == cudaSuccess) e = launch_gather_rows(n, 1, c->ld, stride, c->temp, t->ld, t->temp, t->st);
+    if (e == cudaSuccess) e = launch_gather_rows(n, NPH, c->ld, stride, c->jv, t->ld, t->jv, t->st);
+    if (e == cudaSuccess && c->have_rcn) e = launch_gather_rows(n, 1, c->ld, stride, c->rcn, t->ld, t->rcn, t->st);
+    t->have_rcn = c->have_rcn;
+    t->rconst_valid = false;
+    if (e == cudaSuccess) e = cudaMalloc((void **)&y0, sizeof(double) * NVAR * t->ld);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(y0, t->var, sizeof(double) * NVAR * t->ld, cudaMemcpyDeviceToDevice, t->st);
+    if (e != cudaSuccess) {
+        fail_cuda(c, e, "autotune sample");
+        return fail(RADM2_E_CUDA);
+    }
+    t->timing = true;
+
+    int best = -1;
+    double best_ms = 0.0;
+    long long attempts0 = -1;
+    int count = 0;
+    for (size_t i = 0; i < cands.size(); i++) {
+        const Cand &k = cands[i];
+        t->o.schedule = k.sched;
+        t->o.block_threads = k.bs;
+        t->o.placement = k.place;
+        t->o.min_blocks = k.minb;
+        t->o.blocks_per_sm = 0;
+        drop_graph(t);
+        double ms = -1.0;
+        long long att = -1;
+        if (cudaMemcpyAsync(t->var, y0, sizeof(double) * NVAR * t->ld, cudaMemcpyDeviceToDevice, t->st) ==
+            cudaSuccess) {
+            double rpar[20];
+            int ipar[20];
+            std::memcpy(rpar, RPAR, sizeof rpar);
+            std::memcpy(ipar, IPAR, sizeof ipar);
+            if (rpar[2] == 0.0) rpar[2] = 0.01 * dt;
+            double kms0 = 0.0;
+            int kl0 = 0;
+            radm2_get_kernel_time(t, &kms0, &kl0);  // reset the accumulators
+            const int ierr = radm2_rosenbrock(t, 0.0, dt, AbsTol, RelTol, rpar, ipar);
+            double kms = 0.0;
+            int kl = 0;
+            if (ierr == 1 && radm2_get_kernel_time(t, &kms, &kl) == RADM2_OK && kl == 1) {
+                ms = kms;
+                att = (long long)ipar[13] + ipar[14];
+            }
+        }
+        (void)cudaGetLastError();  // a variant that cannot run here is skipped, not fatal
+        if (ms >= 0.0 && attempts0 < 0) attempts0 = att;
+        const bool same = ms >= 0.0 && att == attempts0;
+        if (same && (best < 0 || ms < best_ms)) {
+            best = (int)i;
+            best_ms = ms;
+        }
+        if (count < table_len) {
+            radm2_tune_entry &te = table[count];
+            te.schedule = k.sched;
+            te.block_threads = k.bs;
+            te.placement = k.place;
+            te.min_blocks = k.minb;
+            te.ms = same ? ms : -1.0;
+            te.attempts = att;
+        }
+        count++;
+    }
+    if (n_entries) *n_entries = count;
+    cudaFree(y0);
+    y0 = nullptr;
+    radm2_destroy(t);
+    if (best < 0) {
+        c->err = "autotune: no solver variant ran on this device";
+        return RADM2_E_CUDA;
+    }
+    drop_graph(c);
+    c->o.schedule = cands[best].sched;
+    c->o.block_threads = cands[best].bs;
+    c->o.placement = cands[best].place;
+    c->o.min_blocks = cands[best].minb;
+    c->o.blocks_per_sm = 0;
+    return RADM2_OK;
+}
 
 size_t radm2_device_bytes(const radm2_ctx *c)
 {

@@ -25,6 +25,8 @@ cudaError_t launch_rconst(int n, int ld, const double *jv, const double *temp, c
                           const double *rcn2o5, double *rconst, cudaStream_t st);
 cudaError_t launch_aos_to_soa(int n, int m, int ld, const double *aos, double *soa, cudaStream_t st);
 cudaError_t launch_soa_to_aos(int n, int m, int ld, const double *soa, double *aos, cudaStream_t st);
+cudaError_t launch_gather_rows(int n, int m, int lds, int stride, const double *src, int ldd, double *dst,
+                               cudaStream_t st);
 cudaError_t launch_fun(int n, int ld, const double *var, const double *fix, const double *rconst, double *vdot,
                        cudaStream_t st);
 cudaError_t launch_jac(int n, int ld, const double *var, const double *fix, const double *rconst, double *jvs,
@@ -33,6 +35,12 @@ cudaError_t launch_decomp_solve(int n, int ld, int fp32, double *g, double *x, i
 size_t reduce_partials_bytes();
 cudaError_t launch_reduce(int n, const int *status, const int *nacc, const int *nrej, const double *texit,
                           const double *hexit, void *partials, RunResult *out, cudaStream_t st);
+
+// (block size, placement, min resident blocks per SM) lists of the built solver variants,
+// per precision (each built for both schedules).  A min-blocks value above 1 caps the
+// registers per thread (65536 / (bs * minb)) for occupancy.
+#define RADM2_VARIANTS_FP64(X) X(64, 0, 1) X(128, 0, 1) X(256, 0, 1) X(128, 0, 3) X(128, 0, 4) X(32, 1, 1) X(32, 3, 1)
+#define RADM2_VARIANTS_FP32(X) X(64, 0, 1) X(128, 0, 1) X(256, 0, 1) X(128, 0, 3) X(128, 0, 4) X(32, 1, 1) X(64, 1, 1) X(32, 3, 1)
 
 // Static properties of one solver variant on the current device.
 struct SolverInfo {

@@ -261,6 +261,26 @@ cudaError_t launch_soa_to_aos(int n, int m, int ld, const double *soa, double *a
     return cudaGetLastError();
 }
 
+// dst[r][i] = src[r][i * stride] for r < m, i < n (struct-of-arrays rows, leading
+// dimensions lds / ldd): a strided sample of cells.
+__global__ void k_gather_rows(int n, int m, int lds, int stride, const double *__restrict__ src, int ldd,
+                              double *__restrict__ dst)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int r = blockIdx.y;
+    if (i < n && r < m) dst[(size_t)r * ldd + i] = src[(size_t)r * lds + (size_t)i * stride];
+}
+
+cudaError_t launch_gather_rows(int n, int m, int lds, int stride, const double *src, int ldd, double *dst,
+                               cudaStream_t st)
+{
+    if (n <= 0 || m <= 0) return cudaSuccess;
+    dim3 grid((n + 255) / 256, m);
+    (void)cudaGetLastError();
+    k_gather_rows<<<grid, 256, 0, st>>>(n, m, lds, stride, src, ldd, dst);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_fun(int n, int ld, const double *var, const double *fix, const double *rconst, double *vdot,
                        cudaStream_t st)
 {

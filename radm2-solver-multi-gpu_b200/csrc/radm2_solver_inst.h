@@ -53,10 +53,8 @@ int check_one()
 
 }  // namespace radm2
 
-// (block size, placement, min resident blocks per SM) lists per precision.  A min-blocks
-// value above 1 caps the registers per thread (65536 / (bs * minb)) for occupancy.
-#define RADM2_VARIANTS_FP64(X) X(64, 0, 1) X(128, 0, 1) X(256, 0, 1) X(128, 0, 3) X(128, 0, 4) X(32, 1, 1) X(32, 3, 1)
-#define RADM2_VARIANTS_FP32(X) X(64, 0, 1) X(128, 0, 1) X(256, 0, 1) X(128, 0, 3) X(128, 0, 4) X(32, 1, 1) X(64, 1, 1) X(32, 3, 1)
+// The built (block size, placement, min blocks) lists, RADM2_VARIANTS_FP64 / _FP32, are in
+// radm2_internal.h (the autotuner walks them too).
 
 #define RADM2_KEY(BS_, PL_, MB_) ((BS_) * 64 + (MB_) * 4 + (PL_))
 #define RADM2_CASE_LAUNCH(BS_, PL_, MB_) \

@@ -35,6 +35,11 @@ class Opts(ctypes.Structure):
                 ("float_coeffs", ctypes.c_int), ("placement", ctypes.c_int), ("min_blocks", ctypes.c_int)]
 
 
+class TuneEntry(ctypes.Structure):
+    _fields_ = [("schedule", ctypes.c_int), ("block_threads", ctypes.c_int), ("placement", ctypes.c_int),
+                ("min_blocks", ctypes.c_int), ("ms", ctypes.c_double), ("attempts", ctypes.c_longlong)]
+
+
 class Stats(ctypes.Structure):
     _fields_ = [("n_accepted", ctypes.c_longlong), ("n_rejected", ctypes.c_longlong),
                 ("n_failed", ctypes.c_longlong), ("worst_status", ctypes.c_int), ("max_steps_cell", ctypes.c_int),
@@ -90,6 +95,11 @@ SIGNATURES = {
                                         ctypes.c_int]),
     "radm2_attach_mlp": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]),
     "radm2_get_ncell": (ctypes.c_int, [ctypes.c_void_p]),
+    "radm2_get_opts": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Opts)]),
+    "radm2_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.POINTER(ctypes.c_double),
+                                      ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                      ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.POINTER(TuneEntry),
+                                      ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     "radm2_device_bytes": (ctypes.c_size_t, [ctypes.c_void_p]),
     "radm2_rosenbrock_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                                                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double,
@@ -302,6 +312,25 @@ class Solver:
         out = np.empty((self.ncell, NFEAT), dtype=np.float32)
         self._check(self.lib.radm2_get_features(self.h, dt, out.ctypes.data_as(_F)))
         return out
+
+    def opts(self):
+        """The options in force (the autotuner rewrites schedule / block shape / placement)."""
+        o = Opts()
+        self._check(self.lib.radm2_get_opts(self.h, ctypes.byref(o)))
+        return {k: getattr(o, k) for k, _ in Opts._fields_}
+
+    def autotune(self, dt, atol, rtol, rpar=None, ipar=None, sample_cells=0):
+        """Time every built variant on a strided sample of the current cells for one split;
+        keep the fastest.  Returns the candidate table (ms = -1: did not run)."""
+        if rpar is None or ipar is None:
+            ipar, rpar = default_params()
+        atol, rtol = _c64(atol), _c64(rtol)
+        rpar, ipar = _c64(rpar), np.ascontiguousarray(ipar, dtype=np.int32)
+        tab = (TuneEntry * 64)()
+        n = ctypes.c_int()
+        self._check(self.lib.radm2_autotune(self.h, dt, _dp(atol), _dp(rtol), _dp(rpar), _ip(ipar), sample_cells,
+                                            tab, 64, ctypes.byref(n)))
+        return [{k: getattr(tab[i], k) for k, _ in TuneEntry._fields_} for i in range(min(n.value, 64))]
 
     def attach_mlp(self, mlp, order=False):
         """Seed every following integration from the network (None detaches)."""

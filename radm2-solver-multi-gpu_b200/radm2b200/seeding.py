@@ -104,6 +104,22 @@ def train_default(device=0, dt=600.0, log=None):
                  "h0_safety": H0_SAFETY}
 
 
+def save_net(net, path, h0_scale=H0_SAFETY):
+    """Store a trained network (parameters, normalisation, seeding scale) as .npz."""
+    xm, xs, ym, ys = net.norm
+    np.savez(path, params=net.params(), xmean=xm, xstd=xs, ymean=ym, ystd=ys, h0_scale=np.float32(h0_scale))
+
+
+def load_net(path, device=0):
+    """A network stored by save_net, ready to seed."""
+    d = np.load(path)
+    net = Mlp(seed=0, device=device)
+    net.set_params(d["params"])
+    net.set_norm(d["xmean"], d["xstd"], d["ymean"], d["ystd"])
+    net.set_h0_scale(float(d["h0_scale"]))
+    return net
+
+
 def evaluate_split_loop(cells, nsplit, dt=600.0, net=None, precision=PREC_FP64, schedule=SCHED_PERSISTENT,
                         use_h0=True, use_order=True, timer=None, safety=None, carry=False, attach=False):
     """Integrate nsplit consecutive splits; with a network, seed every split from it

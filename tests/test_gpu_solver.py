@@ -207,3 +207,30 @@ def test_kernel_timing_with_and_without_graph():
             ms, n = s.kernel_time()
             assert n == 2 and ms > 0.0, (use_graph, ms, n)
 
+
+
+def test_autotune_picks_fastest_and_keeps_results():
+    """The autotuner times every built variant of the context's precision on a sample of its
+    cells, keeps the fastest, leaves the cells untouched, and the tuned context integrates
+    to the same answer as the untuned one."""
+    cells = inputs.make_cells(65536, 6, "mixed")
+    atol, rtol = np.ones(59), np.full(59, 1e-3)
+    with radm2b200.Solver() as s:
+        s.set_cells(cells)
+        ipar, rpar = radm2b200.default_params()
+        assert s.run_split(1, 600.0, atol, rtol, rpar, ipar) == 1
+        y_before, acc_before = s.get_state(), int(ipar[13])
+        s.set_cells(cells)
+        table = s.autotune(600.0, atol, rtol, sample_cells=32768)
+        assert len(table) == 14  # 7 FP64 variants x 2 schedules
+        ran = [t for t in table if t["ms"] > 0]
+        assert len(ran) >= 10 and len({t["attempts"] for t in ran}) == 1
+        best = min(ran, key=lambda t: t["ms"])
+        o = s.opts()
+        assert (o["schedule"], o["block_threads"], o["placement"], o["min_blocks"]) == \
+            (best["schedule"], best["block_threads"], best["placement"], best["min_blocks"])
+        assert np.array_equal(s.get_state(), cells["VAR"])  # the sample ran in a scratch context
+        ipar, rpar = radm2b200.default_params()
+        assert s.run_split(1, 600.0, atol, rtol, rpar, ipar) == 1
+        assert int(ipar[13]) == acc_before
+        assert rel_err(s.get_state(), y_before).max() <= 1e-13
