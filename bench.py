@@ -245,7 +245,7 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     import radm2b200
-    from radm2b200 import inputs, seeding
+    from radm2b200 import inputs, seeding, shard
 
     ncell, seed, wl, night, dt = WORKLOADS[args.workload]
     learned = args.method == "learned"
@@ -322,6 +322,7 @@ def main():
         el_ms = ev0.elapsed_time(ev1)
         kms, klaunch = solver.kernel_time()
         el_ms, kms = max_over_ranks(el_ms, kms)
+        shard.reduce_counters(ipar, dist)  # step counters summed over ranks (outside the timed region)
         return {"el_ms": el_ms, "kms": kms, "klaunch": klaunch, "acc": int(ipar[13]), "rej": int(ipar[14]),
                 "clocks": clocks.summary(), "y0": y0, "tuned": tuned}
 
@@ -413,7 +414,8 @@ def main():
 
     fp64_peak, fp32_peak = radm2b200.fma_peak(local)
     kms, klaunch = main_arm["kms"], main_arm["klaunch"]
-    flops = flops_of(main_arm["acc"], main_arm["rej"], args.precision, refine)
+    # per GPU: the counters are summed over ranks, the kernel time is one rank's (the max)
+    flops = flops_of(main_arm["acc"], main_arm["rej"], args.precision, refine) / world
     per_launch_flops = flops / max(klaunch, 1)
     achieved = per_launch_flops / (kms / max(klaunch, 1) * 1e-3) * 1e-12 if kms > 0 else None
     traffic, traffic_gbs = None, None
@@ -428,7 +430,7 @@ def main():
         if key in tr:
             # DRAM bytes per step attempt from one ncu capture (small case), scaled to the
             # attempts of an average launch here: traffic grows with attempts, not cells
-            att = (main_arm["acc"] + main_arm["rej"]) / max(klaunch, 1)
+            att = (main_arm["acc"] + main_arm["rej"]) / world / max(klaunch, 1)
             traffic = tr[key]["dram_bytes_per_attempt"] * att
             if kms > 0:
                 traffic_gbs = traffic / (kms / max(klaunch, 1) * 1e-3) / 1e9
@@ -462,8 +464,8 @@ def main():
                      "kernel_ms_per_launch": kms / max(klaunch, 1), "flops_per_launch": per_launch_flops,
                      "traffic_gbs": traffic_gbs,
                      "traffic_frac_of_hbm": (traffic_gbs / hbm) if (traffic_gbs and hbm) else None},
-        "steps_per_cell": {"accepted": main_arm["acc"] / ncell / args.steps,
-                           "rejected": main_arm["rej"] / ncell / args.steps},
+        "steps_per_cell": {"accepted": main_arm["acc"] / (ncell * world) / args.steps,
+                           "rejected": main_arm["rej"] / (ncell * world) / args.steps},
         "clocks": main_arm["clocks"],
         "e2e": e2e,
     }
