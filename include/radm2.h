@@ -110,6 +110,9 @@ int radm2_set_inputs(radm2_ctx *ctx, int ncell, const double *VAR, const double 
 /* Species state only (VAR[ncell][59]); the cell count must match set_inputs. */
 int radm2_set_state(radm2_ctx *ctx, const double *VAR);
 int radm2_get_state(radm2_ctx *ctx, double *VAR);
+/* Copy the current per-cell inputs back to host arrays in the reference layout (any
+ * pointer may be NULL to skip that array). */
+int radm2_get_inputs(radm2_ctx *ctx, double *VAR, double *FIX, double *TEMP, double *RC_N2O5, double *JV);
 
 /* Same inputs, already in device memory in struct-of-arrays layout:
  * var[59][ld], fix[2][ld], temp[ld], rc_n2o5[ld] (NULL = zero), jv[28][ld], with
@@ -187,6 +190,27 @@ int radm2_fma_peak(int device, double *fp64_tflops, double *fp32_tflops);
 
 /* Number of cells and device bytes held by the context. */
 int radm2_get_ncell(const radm2_ctx *ctx);
+
+/* WRF -> KPP conversion, replacing dev_convert + convertWRFChemData (mgpu.cu:513-706).
+ * WRF fields are field-major with i fastest, field[f][nj][nk][ni]; the window
+ * [i0, i0+wi) x [k0, k0+wk) x [j0, j0+wj) becomes the context's cells, cell
+ * p = (j'*wk + k')*wi + i' (the reference launch order).  Fields read: ph 0..27 (J per
+ * minute), chem and rad (the species map of mgpu.cu:586-644, chem 0..43, rad 0..27),
+ * phy 0 pressure (Pa), 1 temperature (K), 2 air density (kg/m3), moist 1 water vapour
+ * (kg/kg).  Sets VAR (ppmV -> molec/cm3, negatives clamped to 0), FIX {H2O, M}, TEMP,
+ * RC_N2O5 (per cell) and JV (per second); the rate constants are recomputed on the next
+ * integration.  radm2_wrf_grid_default gives the reference's 48 x 20 x 48 domain with its
+ * 39 x 19 x 39 window (28,899 cells). */
+typedef struct radm2_wrf_grid {
+    int ni, nk, nj; /* field dimensions */
+    int i0, k0, j0; /* window origin */
+    int wi, wk, wj; /* window extent */
+} radm2_wrf_grid;
+int radm2_wrf_grid_default(radm2_wrf_grid *grid);
+int radm2_convert_wrf(radm2_ctx *ctx, const radm2_wrf_grid *grid, const double *ph, const double *chem,
+                      const double *rad, const double *phy, const double *moist);        /* host fields */
+int radm2_convert_wrf_device(radm2_ctx *ctx, const radm2_wrf_grid *grid, const double *ph, const double *chem,
+                             const double *rad, const double *phy, const double *moist); /* device fields */
 int radm2_get_opts(const radm2_ctx *ctx, radm2_opts *out);  /* options in force (after autotune) */
 
 /* Autotuner (no counterpart in the reference, which has one fixed launch shape).  Times

@@ -15,6 +15,7 @@ This recipe cuts these functions out of mgpu.cu where it lies, unmodified:
     dev_Jac_SP                               mgpu.cu:1672-2652
     dev_KppDecomp                            mgpu.cu:2726-2780
     dev_KppSolve                             mgpu.cu:2854-3096
+    dev_convert (WRF -> KPP conversion)      mgpu.cu:513-646
 
 and compiles them with g++ for one cell per call, behind the shim in
 oracle/ref_harness.cpp (CUDA qualifiers as no-ops, blockIdx/threadIdx as
@@ -45,11 +46,13 @@ FUNCTIONS = [
     r"__global__\s+void\s+dev_Jac_SP\s*\(",
     r"__global__\s+void\s+dev_KppDecomp\s*\(",
     r"__global__\s+void\s+dev_KppSolve\s*\(",
+    r"__global__\s+void\s+dev_convert\s*\(",
 ]
 
 # Object-like and function-like #defines from the reference's header block that the
 # extracted functions use (sizes, species indices, min/max/abs macros).
-DEFINE_RE = re.compile(r"^#define\s+(NSPEC|NVAR|NVARACT|NFIX|NREACT|NVARST|NFIXST|NONZERO|LU_NONZERO|CNVAR|"
+DEFINE_RE = re.compile(r"^#define\s+(NSPEC|NVAR|NVARACT|NFIX|NREACT|NVARST|NFIXST|NONZERO|LU_NONZERO|CNVAR|NPH|"
+                       r"navgdro|mwh|mwo|mwair|mwh2o|dens2con_a|dens2con_w|"
                        r"ind_\w+|indf_\w+|Pj_\w+|ZERO|ONE|TWO|HALF|THREE_HUNDRED|DeltaMin|MAX|MIN|ABS|SQRT)\b")
 
 

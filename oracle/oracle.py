@@ -50,6 +50,35 @@ def _c(a, shape):
 _lib = None
 
 
+class WrfGrid(ctypes.Structure):
+    """WRF field dimensions (i fastest) and the interior window converted to cells."""
+    _fields_ = [(k, ctypes.c_int) for k in ("ni", "nk", "nj", "i0", "k0", "j0", "wi", "wk", "wj")]
+
+
+# The reference's domain and window (mgpu.cu:513-536, 682-706).
+REF_WRF_GRID = (48, 20, 48, 4, 0, 4, 39, 19, 39)
+
+
+def _wrf_outputs(g):
+    n = g.wi * g.wk * g.wj
+    return {"VAR": np.zeros((n, NVAR)), "FIX": np.zeros((n, NFIX)), "TEMP": np.zeros(n), "RC_N2O5": np.zeros(n),
+            "JV": np.zeros((n, NPH))}
+
+
+def _wrf_fields(fields):
+    return [np.ascontiguousarray(fields[k], dtype=np.float64) for k in ("ph", "chem", "rad", "phy", "moist")]
+
+
+def convert_wrf(fields, grid=REF_WRF_GRID):
+    """WRF fields (dict ph/chem/rad/phy/moist, each [nfield][nj][nk][ni]) -> per-cell inputs."""
+    g = WrfGrid(*grid)
+    out = _wrf_outputs(g)
+    f = _wrf_fields(fields)
+    lib().orc_convert_wrf(ctypes.byref(g), *[_dp(a) for a in f],
+                          *[_dp(out[k]) for k in ("VAR", "FIX", "TEMP", "RC_N2O5", "JV")])
+    return out
+
+
 def lib():
     global _lib
     if _lib is None:
@@ -72,6 +101,7 @@ def lib():
         L.orc_parse_params.argtypes = [ctypes.c_double, ctypes.c_double, _D, _D, _D, _I, ctypes.c_int,
                                        ctypes.POINTER(Params)]
         L.orc_parse_params.restype = ctypes.c_int
+        L.orc_convert_wrf.argtypes = [ctypes.POINTER(WrfGrid), _D, _D, _D, _D, _D, _D, _D, _D, _D, _D]
         _lib = L
     return _lib
 
@@ -172,6 +202,7 @@ def ref():
         R.ref_decomp.argtypes = [_D]
         R.ref_decomp.restype = ctypes.c_int
         R.ref_solve.argtypes = [_D, _D]
+        R.ref_convert_wrf.argtypes = [_D] * 10
         _ref = R
     return _ref
 
@@ -208,3 +239,12 @@ def ref_solve(LU, X):
     LU, X = _c(LU, (NJVS,)), _c(X, (NVAR,)).copy()
     ref().ref_solve(_dp(LU), _dp(X))
     return X
+
+
+def ref_convert_wrf(fields):
+    """The reference's dev_convert over its own launch (the 48 x 20 x 48 domain only)."""
+    g = WrfGrid(*REF_WRF_GRID)
+    out = _wrf_outputs(g)
+    f = _wrf_fields(fields)
+    ref().ref_convert_wrf(*[_dp(a) for a in f], *[_dp(out[k]) for k in ("VAR", "FIX", "TEMP", "RC_N2O5", "JV")])
+    return out

@@ -266,6 +266,48 @@ void orc_rconst_batch(int ncell, const double *JV, const double *TEMP, const dou
                    RCT + (size_t)c * ORC_NREACT);
 }
 
+/* ---------------------------------------------------------------- WRF -> KPP */
+
+/* mgpu.cu:29-44: molecules per mole, molecular weights, density -> concentration. */
+#define ORC_NAVGDRO (6.022e23)
+#define ORC_MWAIR (28.97)
+#define ORC_MWH2O (2 * (1.0079) + (15.9994))
+#define ORC_DENS2CON_A (1.0e-3 * (1.0 / ORC_MWAIR) * ORC_NAVGDRO)
+#define ORC_DENS2CON_W (1.0e-3 * (1.0 / ORC_MWH2O) * ORC_NAVGDRO)
+
+void orc_convert_wrf(const orc_wrf_grid *g, const double *ph, const double *chem, const double *rad,
+                     const double *phy, const double *moist, double *VAR, double *FIX, double *TEMP,
+                     double *RC_N2O5, double *JV)
+{
+    const size_t fs = (size_t)g->nj * g->nk * g->ni; /* one field */
+    const int n = g->wi * g->wk * g->wj;
+    for (int p = 0; p < n; p++) {
+        const int ii = p % g->wi, kk = (p / g->wi) % g->wk, jj = p / (g->wi * g->wk);
+        const size_t o = ((size_t)(g->j0 + jj) * g->nk + (g->k0 + kk)) * g->ni + (g->i0 + ii);
+        const double pres = phy[o], t = phy[fs + o], rho = phy[2 * fs + o], qv = moist[fs + o];
+        double *v = VAR + (size_t)p * ORC_NVAR;
+        /* mgpu.cu:539-552 */
+        FIX[(size_t)p * ORC_NFIX + 1] = ORC_DENS2CON_A * rho;
+        FIX[(size_t)p * ORC_NFIX + 0] = ORC_DENS2CON_W * qv * rho;
+        TEMP[p] = t;
+        const double es = 1000. * 0.6112 * exp(17.67 * (t - 273.15) / (t - 29.65));
+        const double qvs = es / (pres - es);
+        double rh = qv / qvs;
+        rh = rh >= 0.0f ? rh : 0.0f;
+        rh = rh < 1.0f ? rh : 1.0f;
+        RC_N2O5[p] = 1.0 / (3.6e4 * exp(-pow((rh / 0.28), 2.8) + 300.0));
+        /* mgpu.cu:555-583: ppmV -> molec/cm3, J per minute -> per second */
+        const double conv = 1.0E-6 * ORC_DENS2CON_A * rho;
+        for (int k = 0; k < ORC_NPH; k++) JV[(size_t)p * ORC_NPH + k] = ph[orc_wrf_jv_src[k] * fs + o] / 60.0;
+        /* mgpu.cu:586-644 */
+        for (int i = 0; i < ORC_NVAR; i++) {
+            const double *src = orc_wrf_var_src[i][0] == 0 ? chem : rad;
+            const double x = src[(size_t)orc_wrf_var_src[i][1] * fs + o];
+            v[i] = conv * (x >= 0.0 ? x : 0.0);
+        }
+    }
+}
+
 /* ---------------------------------------------------------------- Rosenbrock() mirror */
 
 int orc_parse_params(double Tstart, double Tend, const double *AbsTol, const double *RelTol,

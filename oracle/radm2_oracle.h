@@ -16,6 +16,7 @@
  *                                       with KPP's Rosenbrock semantics)
  *   step control     mgpu.cu:3168-3262, time loop mgpu.cu:1595-1614
  *   driver params    mgpu.cu:3664-3848 (orc_rosenbrock: IPAR/RPAR parsing, codes)
+ *   WRF -> KPP       mgpu.cu:513-646   (orc_convert_wrf, tables generated)
  *
  * The mechanism functions are pinned bit-for-bit against the reference's own
  * dev_Update_RCONST / dev_Fun / dev_Jac_SP / dev_KppDecomp / dev_KppSolve,
@@ -103,6 +104,25 @@ int orc_rosenbrock(double Tstart, double Tend, const double *AbsTol, const doubl
 /* Parameter parsing only (returns 1 or a negative code). */
 int orc_parse_params(double Tstart, double Tend, const double *AbsTol, const double *RelTol,
                      const double *RPAR, const int *IPAR, int float_coeffs, orc_params *p);
+
+/* WRF -> KPP conversion (mgpu.cu:513-646).  WRF fields are field-major with i fastest,
+ * field[f][nj][nk][ni]; the window [i0, i0+wi) x [k0, k0+wk) x [j0, j0+wj) becomes cells
+ * p = (j'*wk + k')*wi + i' (the order of the reference's launch, mgpu.cu:682-706).
+ * Fields read: ph 0..27 (J per minute), chem and rad (orc_wrf_var_src), phy 0 pressure
+ * (Pa), 1 temperature (K), 2 air density (kg/m3), moist 1 water vapour (kg/kg).
+ * Outputs in the per-cell layout: VAR[p][59], FIX[p][2] = {H2O, M}, TEMP[p], RC_N2O5[p],
+ * JV[p][28].  TEMP and RC_N2O5 are per cell (the reference writes element 0 for every
+ * cell, mgpu.cu:545, 552: a defect, not the intent). */
+typedef struct orc_wrf_grid {
+    int ni, nk, nj;
+    int i0, k0, j0;
+    int wi, wk, wj;
+} orc_wrf_grid;
+extern const int orc_wrf_var_src[ORC_NVAR][2];
+extern const int orc_wrf_jv_src[ORC_NPH];
+void orc_convert_wrf(const orc_wrf_grid *g, const double *ph, const double *chem, const double *rad,
+                     const double *phy, const double *moist, double *VAR, double *FIX, double *TEMP,
+                     double *RC_N2O5, double *JV);
 
 #ifdef __cplusplus
 }

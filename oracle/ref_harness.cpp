@@ -65,4 +65,27 @@ void ref_solve(const double *jvs, double *x)
     dev_KppSolve(&m1, &m2, 1, (double *)jvs, x);
 }
 
+// dev_convert over the reference's launch (mgpu.cu:682-706): gridDim (19, 39), blockDim 39.
+// The kernel writes *TEMP and *RC_N2O5 without a cell offset; the wrapper hands it the
+// cell's own element so every cell's value is kept.
+void ref_convert_wrf(const double *ph, const double *chem, const double *rad, const double *phy, const double *moist,
+                     double *VAR, double *FIX, double *TEMP, double *RC_N2O5, double *JV)
+{
+    gridDim = {19, 39, 1};
+    blockDim = {39, 1, 1};
+    for (unsigned by = 0; by < 39; by++)
+        for (unsigned bx = 0; bx < 19; bx++)
+            for (unsigned tx = 0; tx < 39; tx++) {
+                blockIdx = {bx, by, 0};
+                threadIdx = {tx, 0, 0};
+                const size_t p = (size_t)by * 19 * 39 + bx * 39 + tx;
+                dev_convert(VAR, FIX, TEMP + p, nullptr, RC_N2O5 + p, JV, (double *)ph, (double *)chem, (double *)rad,
+                            (double *)phy, (double *)moist);
+            }
+    gridDim = {1, 1, 1};
+    blockDim = {1, 1, 1};
+    blockIdx = {0, 0, 0};
+    threadIdx = {0, 0, 0};
+}
+
 }  // extern "C"

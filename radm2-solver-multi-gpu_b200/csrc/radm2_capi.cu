@@ -11,6 +11,7 @@
 
 #include "../../include/radm2.h"
 #include "radm2_internal.h"
+#include "gen/radm2_wrf.h"
 
 using namespace radm2;
 
@@ -557,6 +558,22 @@ int radm2_get_state(radm2_ctx *c, double *VAR)
     return download_aos(c, c->var, NVAR, VAR);
 }
 
+int radm2_get_inputs(radm2_ctx *c, double *VAR, double *FIX, double *TEMP, double *RC_N2O5, double *JV)
+{
+    if (!valid_ctx(c)) return RADM2_E_ARG;
+    if (!c->var) return RADM2_E_STATE;
+    int rc = RADM2_OK;
+    if (VAR && (rc = download_aos(c, c->var, NVAR, VAR))) return rc;
+    if (FIX && (rc = download_aos(c, c->fix, NFIX, FIX))) return rc;
+    if (TEMP && (rc = download_aos(c, c->temp, 1, TEMP))) return rc;
+    if (RC_N2O5) {
+        if (!c->have_rcn) return RADM2_E_STATE;  // inputs came without rc_n2o5 (formula used)
+        if ((rc = download_aos(c, c->rcn, 1, RC_N2O5))) return rc;
+    }
+    if (JV && (rc = download_aos(c, c->jv, NPH, JV))) return rc;
+    return RADM2_OK;
+}
+
 int radm2_set_inputs_device(radm2_ctx *c, int ncell, int ld, const double *var, const double *fix,
                             const double *temp, const double *rc_n2o5, const double *jv)
 {
@@ -792,6 +809,65 @@ int radm2_get_kernel_time(radm2_ctx *c, double *ms, int *launches)
     *launches = c->kernel_launches;
     c->kernel_ms = 0.0;
     c->kernel_launches = 0;
+    return RADM2_OK;
+}
+
+// ---------------------------------------------------------------- WRF -> KPP conversion
+
+int radm2_wrf_grid_default(radm2_wrf_grid *g)
+{
+    if (!g) return RADM2_E_ARG;
+    const int init[9] = RADM2_WRF_REF_GRID_INIT;
+    std::memcpy(g, init, sizeof init);
+    return RADM2_OK;
+}
+
+static bool wrf_grid_ok(const radm2_wrf_grid *g)
+{
+    return g && g->ni > 0 && g->nk > 0 && g->nj > 0 && g->wi > 0 && g->wk > 0 && g->wj > 0 && g->i0 >= 0 &&
+           g->k0 >= 0 && g->j0 >= 0 && g->i0 + g->wi <= g->ni && g->k0 + g->wk <= g->nk && g->j0 + g->wj <= g->nj &&
+           (long long)g->wi * g->wk * g->wj <= (1LL << 30) && (long long)g->ni * g->nk * g->nj <= (1LL << 31);
+}
+
+int radm2_convert_wrf_device(radm2_ctx *c, const radm2_wrf_grid *g, const double *ph, const double *chem,
+                             const double *rad, const double *phy, const double *moist)
+{
+    if (!valid_ctx(c) || !wrf_grid_ok(g) || !ph || !chem || !rad || !phy || !moist) return RADM2_E_ARG;
+    CK(cudaSetDevice(c->o.device));
+    int rc = ensure_cells(c, g->wi * g->wk * g->wj);
+    if (rc) return rc;
+    WrfGrid wg;
+    std::memcpy(&wg, g, sizeof wg);
+    CK(launch_convert_wrf(wg, ph, chem, rad, phy, moist, c->ld, c->var, c->fix, c->temp, c->rcn, c->jv, c->st));
+    c->have_rcn = true;
+    c->rconst_valid = false;
+    return RADM2_OK;
+}
+
+int radm2_convert_wrf(radm2_ctx *c, const radm2_wrf_grid *g, const double *ph, const double *chem, const double *rad,
+                      const double *phy, const double *moist)
+{
+    if (!valid_ctx(c) || !wrf_grid_ok(g) || !ph || !chem || !rad || !phy || !moist) return RADM2_E_ARG;
+    CK(cudaSetDevice(c->o.device));
+    // only the fields the conversion reads travel: ph 0..27, chem / rad up to the last
+    // mapped field, phy 0..2, moist 0..1
+    const size_t fs = (size_t)g->ni * g->nk * g->nj;
+    const int counts[5] = {RADM2_WRF_NPH_USED, RADM2_WRF_NCHEM_USED, RADM2_WRF_NRAD_USED, 3, 2};
+    const double *src[5] = {ph, chem, rad, phy, moist};
+    size_t total = 0;
+    for (int f = 0; f < 5; f++) total += counts[f] * fs;
+    int rc = ensure_stage(c, total * sizeof(double));
+    if (rc) return rc;
+    const double *dev[5];
+    size_t off = 0;
+    for (int f = 0; f < 5; f++) {
+        CK(cudaMemcpyAsync(c->stage + off, src[f], counts[f] * fs * sizeof(double), cudaMemcpyHostToDevice, c->st));
+        dev[f] = c->stage + off;
+        off += counts[f] * fs;
+    }
+    rc = radm2_convert_wrf_device(c, g, dev[0], dev[1], dev[2], dev[3], dev[4]);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(c->st));  // the staging buffer is reused by the next upload
     return RADM2_OK;
 }
 

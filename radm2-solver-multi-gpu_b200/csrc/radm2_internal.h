@@ -25,6 +25,15 @@ cudaError_t launch_rconst(int n, int ld, const double *jv, const double *temp, c
                           const double *rcn2o5, double *rconst, cudaStream_t st);
 cudaError_t launch_aos_to_soa(int n, int m, int ld, const double *aos, double *soa, cudaStream_t st);
 cudaError_t launch_soa_to_aos(int n, int m, int ld, const double *soa, double *aos, cudaStream_t st);
+// WRF field dimensions (i fastest) and the converted window; mirrors radm2_wrf_grid.
+struct WrfGrid {
+    int ni, nk, nj;
+    int i0, k0, j0;
+    int wi, wk, wj;
+};
+cudaError_t launch_convert_wrf(const WrfGrid &g, const double *ph, const double *chem, const double *rad,
+                               const double *phy, const double *moist, int ld, double *var, double *fix,
+                               double *temp, double *rcn, double *jv, cudaStream_t st);
 cudaError_t launch_gather_rows(int n, int m, int lds, int stride, const double *src, int ldd, double *dst,
                                cudaStream_t st);
 cudaError_t launch_fun(int n, int ld, const double *var, const double *fix, const double *rconst, double *vdot,

@@ -3,6 +3,7 @@
 // per-cell outcomes into the IPAR/RPAR aggregates.
 #include "radm2_device.cuh"
 #include "radm2_internal.h"
+#include "gen/radm2_wrf.h"
 
 namespace radm2 {
 
@@ -258,6 +259,61 @@ cudaError_t launch_soa_to_aos(int n, int m, int ld, const double *soa, double *a
     dim3 grid((n + 31) / 32, (m + 31) / 32), block(32, 8);
     (void)cudaGetLastError();
     k_soa_to_aos<<<grid, block, 0, st>>>(n, m, ld, soa, aos);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- WRF -> KPP conversion
+// mgpu.cu:513-646 (dev_convert), one thread per cell of the window, writing the context's
+// struct-of-arrays inputs directly.  Expressions as the reference writes them (this file
+// is built without FMA contraction); TEMP and RC_N2O5 per cell.
+#define RADM2_NAVGDRO (6.022e23)
+#define RADM2_MWAIR (28.97)
+#define RADM2_MWH2O (2 * (1.0079) + (15.9994))
+#define RADM2_DENS2CON_A (1.0e-3 * (1.0 / RADM2_MWAIR) * RADM2_NAVGDRO)
+#define RADM2_DENS2CON_W (1.0e-3 * (1.0 / RADM2_MWH2O) * RADM2_NAVGDRO)
+
+__global__ void k_convert_wrf(const WrfGrid g, const double *__restrict__ ph, const double *__restrict__ chem,
+                              const double *__restrict__ rad, const double *__restrict__ phy,
+                              const double *__restrict__ moist, int ld, double *__restrict__ var,
+                              double *__restrict__ fix, double *__restrict__ temp, double *__restrict__ rcn,
+                              double *__restrict__ jv)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= g.wi * g.wk * g.wj) return;
+    const size_t fs = (size_t)g.nj * g.nk * g.ni;
+    const int ii = p % g.wi, kk = (p / g.wi) % g.wk, jj = p / (g.wi * g.wk);
+    const size_t o = ((size_t)(g.j0 + jj) * g.nk + (g.k0 + kk)) * g.ni + (g.i0 + ii);
+    const double pres = phy[o], t = phy[fs + o], rho = phy[2 * fs + o], qv = moist[fs + o];
+    fix[(size_t)ld + p] = RADM2_DENS2CON_A * rho;
+    fix[p] = RADM2_DENS2CON_W * qv * rho;
+    temp[p] = t;
+    const double es = 1000. * 0.6112 * exp(17.67 * (t - 273.15) / (t - 29.65));
+    const double qvs = es / (pres - es);
+    double rh = qv / qvs;
+    rh = rh >= 0.0f ? rh : 0.0f;
+    rh = rh < 1.0f ? rh : 1.0f;
+    rcn[p] = 1.0 / (3.6e4 * exp(-pow((rh / 0.28), 2.8) + 300.0));
+    const double conv = 1.0E-6 * RADM2_DENS2CON_A * rho;
+#define RADM2_JV_OUT(k, f) jv[(size_t)(k) * ld + p] = ph[(size_t)(f) * fs + o] / 60.0;
+    RADM2_WRF_JV_SRC(RADM2_JV_OUT)
+#undef RADM2_JV_OUT
+#define RADM2_VAR_OUT(v, src, f)                                             \
+    {                                                                        \
+        const double x_ = ((src) == 0 ? chem : rad)[(size_t)(f) * fs + o];   \
+        var[(size_t)(v) * ld + p] = conv * (x_ >= 0.0 ? x_ : 0.0);          \
+    }
+    RADM2_WRF_VAR_SRC(RADM2_VAR_OUT)
+#undef RADM2_VAR_OUT
+}
+
+cudaError_t launch_convert_wrf(const WrfGrid &g, const double *ph, const double *chem, const double *rad,
+                               const double *phy, const double *moist, int ld, double *var, double *fix,
+                               double *temp, double *rcn, double *jv, cudaStream_t st)
+{
+    const int n = g.wi * g.wk * g.wj;
+    if (n <= 0) return cudaSuccess;
+    (void)cudaGetLastError();
+    k_convert_wrf<<<(n + 127) / 128, 128, 0, st>>>(g, ph, chem, rad, phy, moist, ld, var, fix, temp, rcn, jv);
     return cudaGetLastError();
 }
 

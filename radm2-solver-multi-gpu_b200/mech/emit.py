@@ -503,7 +503,35 @@ def emit_oracle(m, out_dir):
     for s, t in enumerate(m["jvs"]):
         c.append("  JVS[%d] = %s;\n" % (s, r(t)))
     c.append("}\n")
+    w = m["wrf"]
+    src_id = {"chem": 0, "rad": 1}
+    c.append("\n/* WRF -> KPP conversion tables, mgpu.cu:513-646 (dev_convert): species i takes field\n"
+             " * orc_wrf_var_src[i][1] of the chem (0) or rad (1) array; jv k takes ph field orc_wrf_jv_src[k]. */\n")
+    c.append("const int orc_wrf_var_src[%d][2] = {%s};\n" % (
+        len(w["var_src"]), ",".join("{%d,%d}" % (src_id[a], f) for a, f in w["var_src"])))
+    c.append("const int orc_wrf_jv_src[%d] = {%s};\n" % (len(w["jv_src"]), ",".join(map(str, w["jv_src"]))))
     write(os.path.join(out_dir, "radm2_oracle_gen.c"), c)
+
+
+def emit_wrf(m, out_dir):
+    """WRF -> KPP conversion tables for the kernels (mgpu.cu:513-646, 682-706)."""
+    w = m["wrf"]
+    src_id = {"chem": 0, "rad": 1}
+    d, g = w["dims"], w["window"]
+    h = [BANNER, "#pragma once\n/* WRF -> KPP conversion, %s.\n"
+         " * Fields are field-major with i fastest: field[f][nj][nk][ni].  Species v takes\n"
+         " * conv * max(src[f], 0) with src 0 = chem, 1 = rad; photolysis slot k takes ph[f] / 60. */\n"
+         % w["citation"]]
+    h.append("#define RADM2_WRF_VAR_SRC(X) %s\n" % " ".join("X(%d,%d,%d)" % (v, src_id[a], f)
+                                                          for v, (a, f) in enumerate(w["var_src"])))
+    h.append("#define RADM2_WRF_JV_SRC(X) %s\n" % " ".join("X(%d,%d)" % (k, f) for k, f in enumerate(w["jv_src"])))
+    h.append("#define RADM2_WRF_NCHEM_USED %d\n" % (1 + max(f for a, f in w["var_src"] if a == "chem")))
+    h.append("#define RADM2_WRF_NRAD_USED %d\n" % (1 + max(f for a, f in w["var_src"] if a == "rad")))
+    h.append("#define RADM2_WRF_NPH_USED %d\n" % (1 + max(w["jv_src"])))
+    h.append("/* the reference's domain (ni, nk, nj) and interior window (i0, k0, j0, wi, wk, wj) */\n")
+    h.append("#define RADM2_WRF_REF_GRID_INIT {%d, %d, %d, %d, %d, %d, %d, %d, %d}\n" % (
+        d["ni"], d["nk"], d["nj"], g["i0"], g["k0"], g["j0"], g["wi"], g["wk"], g["wj"]))
+    write(os.path.join(out_dir, "radm2_wrf.h"), h)
 
 
 def write(path, parts):
@@ -514,6 +542,7 @@ def write(path, parts):
 def main():
     m = load()
     flops = emit_cuda(m, CSRC_GEN)
+    emit_wrf(m, CSRC_GEN)
     emit_oracle(m, ORACLE_GEN)
     print("emitted", CSRC_GEN, ORACLE_GEN, flops)
 

@@ -258,6 +258,34 @@ def main():
     ros_tab["ros_ELO"] = re.search(r"\*ros_ELO\s*=\s*\(double\)\s*([0-9.]+)", ros_body).group(1)
     ros_tab["ros_S"] = int(re.search(r"\*ros_S\s*=\s*(\d+)", ros_body).group(1))
 
+    # WRF -> KPP conversion (dev_convert, mgpu.cu:513-646): which WRF field feeds each
+    # species and photolysis slot, the field dimensions, and the interior window the
+    # launch in convertWRFChemData (mgpu.cu:682-706) covers.
+    conv_body = strip_comments(function_body(src, r"__global__\s+void\s+dev_convert\s*\("))
+    var_src = {}
+    for a, arr, b in re.findall(r"VAR\[MY_I\((\d+)\)\]\s*=\s*conv\s*\*\s*MAX\(\(wrf(chem|rad)data\[\(\((\d+)\)\*",
+                                conv_body):
+        assert int(a) not in var_src
+        var_src[int(a)] = [arr, int(b)]
+    assert sorted(var_src) == list(range(nvar)), "dev_convert must set every species"
+    jv_src = {}
+    for n, m2, div in re.findall(r"jv\[MY_I\((\d+)\)\]\s*=\s*\(wrfphdata\[\(\((\d+)\)\*[^;]*\)\s*/\s*([0-9.]+)\s*;",
+                                 conv_body):
+        assert float(div) == 60.0
+        jv_src[int(n)] = int(m2)
+    assert sorted(jv_src) == list(range(nph))
+    dims = re.search(r"wrfphydata\[\(\(2\)\*(\d+)\*(\d+)\*(\d+) \+ \(j\)\*(\d+)\*(\d+) \+ \(k\)\*(\d+)", conv_body)
+    nj_, nk_, ni_ = int(dims.group(1)), int(dims.group(2)), int(dims.group(3))
+    offs = {v: int(o) for v, o in re.findall(r"\b([ijk])\s*\+=\s*(\d+)\s*;", conv_body)}
+    launch = function_body(src, r"void\s+convertWRFChemData\s*\(")
+    gy = int(re.search(r"gridDim\.y\s*=\s*(\d+)", launch).group(1))
+    gx = int(re.search(r"gridDim\.x\s*=\s*(\d+)", launch).group(1))
+    bx = int(re.search(r"blockDim\.x\s*=\s*(\d+)", launch).group(1))
+    wrf = {"citation": "mgpu.cu:513-646 (dev_convert), 682-706 (convertWRFChemData)",
+           "var_src": [var_src[i] for i in range(nvar)], "jv_src": [jv_src[i] for i in range(nph)],
+           "dims": {"ni": ni_, "nk": nk_, "nj": nj_},
+           "window": {"i0": offs["i"], "k0": offs["k"], "j0": offs["j"], "wi": bx, "wk": gx, "wj": gy}}
+
     # Structural facts used by tests and the emitter.
     lower = sum(1 for s in range(lu_nonzero) if pattern["icol"][s] < pattern["irow"][s])
     upper = sum(1 for s in range(lu_nonzero) if pattern["icol"][s] > pattern["irow"][s])
@@ -281,6 +309,7 @@ def main():
         "jvs": [jvs[i] for i in range(lu_nonzero)],
         "lu": pattern,
         "ros3": ros_tab,
+        "wrf": wrf,
     }
     dst = os.path.join(HERE, "radm2_mech.json")
     with open(dst, "w") as f:

@@ -138,3 +138,42 @@ WORKLOADS = {
     "mixed-4m": (4194304, 2, "mixed", 0.4, 24),
     "mixed-4m-eval": (4194304, 3, "mixed", 0.4, 24),
 }
+
+
+# WRF field sets of the reference's conversion step (mgpu.cu:255-260, 477-484): chem 82,
+# rad 29, ph 28, phy 3, moist 6 fields, each [nj][nk][ni] = [48][20][48] there.
+WRF_NFIELDS = {"chem": 82, "rad": 29, "ph": 28, "phy": 3, "moist": 6}
+
+
+def make_wrf_fields(seed, ni=48, nk=20, nj=48, neg_frac=0.01):
+    """Seeded WRF-like fields, field-major with i fastest: [nfield][nj][nk][ni].
+
+    phy: 0 pressure U(50, 101.3) kPa in Pa, 1 temperature U(220, 310) K, 2 air density
+    p / (287.05 T); moist 1: water vapour 1e-5..2e-2 kg/kg (log-uniform, other moist
+    fields the same); chem / rad: mixing ratios 1e-9..1e-1 ppmV log-uniform, a fraction
+    neg_frac slightly negative (WRF advection undershoots, clamped by the conversion);
+    ph: photolysis rates per minute, J0 * 60 * cos(SZA)^n with SZA U(0, 90) deg per column.
+    Every value is a pure function of (seed, field, point)."""
+    n = ni * nk * nj
+    pts = np.arange(n, dtype=np.uint64)
+    col = (pts % np.uint64(ni)) + np.uint64(ni) * (pts // np.uint64(ni * nk))  # (i, j): one column
+
+    def u(fid, idx=pts):
+        return uniform(seed, idx, 1000 + fid)
+
+    pres = 100.0 * (500.0 + 513.0 * u(1))
+    temp = 220.0 + 90.0 * u(2)
+    rho = pres / (287.05 * temp)
+    phy = np.stack([pres, temp, rho]).reshape(3, nj, nk, ni)
+    qv = _logu(u(3), 1.0e-5, 2.0e-2)
+    moist = np.stack([qv] * WRF_NFIELDS["moist"]).reshape(-1, nj, nk, ni)
+
+    def mixing(fid):
+        x = _logu(u(fid), 1.0e-9, 1.0e-1)
+        return np.where(u(fid + 5000) < neg_frac, -0.1 * x, x)
+
+    chem = np.stack([mixing(100 + f) for f in range(WRF_NFIELDS["chem"])]).reshape(-1, nj, nk, ni)
+    rad = np.stack([mixing(300 + f) for f in range(WRF_NFIELDS["rad"])]).reshape(-1, nj, nk, ni)
+    mu = np.cos(np.deg2rad(90.0 * u(4, col)))
+    ph = np.stack([60.0 * J0[k] * np.power(mu, JN[k]) for k in range(NPH)]).reshape(NPH, nj, nk, ni)
+    return {"ph": ph, "chem": chem, "rad": rad, "phy": phy, "moist": moist}

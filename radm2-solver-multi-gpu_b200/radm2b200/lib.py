@@ -35,6 +35,10 @@ class Opts(ctypes.Structure):
                 ("float_coeffs", ctypes.c_int), ("placement", ctypes.c_int), ("min_blocks", ctypes.c_int)]
 
 
+class WrfGrid(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int) for k in ("ni", "nk", "nj", "i0", "k0", "j0", "wi", "wk", "wj")]
+
+
 class TuneEntry(ctypes.Structure):
     _fields_ = [("schedule", ctypes.c_int), ("block_threads", ctypes.c_int), ("placement", ctypes.c_int),
                 ("min_blocks", ctypes.c_int), ("ms", ctypes.c_double), ("attempts", ctypes.c_longlong)]
@@ -95,6 +99,11 @@ SIGNATURES = {
                                         ctypes.c_int]),
     "radm2_attach_mlp": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]),
     "radm2_get_ncell": (ctypes.c_int, [ctypes.c_void_p]),
+    "radm2_get_inputs": (ctypes.c_int, [ctypes.c_void_p, _D, _D, _D, _D, _D]),
+    "radm2_wrf_grid_default": (ctypes.c_int, [ctypes.POINTER(WrfGrid)]),
+    "radm2_convert_wrf": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(WrfGrid), _D, _D, _D, _D, _D]),
+    "radm2_convert_wrf_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(WrfGrid), ctypes.c_void_p,
+                                                ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "radm2_get_opts": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Opts)]),
     "radm2_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.POINTER(ctypes.c_double),
                                       ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
@@ -311,6 +320,26 @@ class Solver:
     def features(self, dt):
         out = np.empty((self.ncell, NFEAT), dtype=np.float32)
         self._check(self.lib.radm2_get_features(self.h, dt, out.ctypes.data_as(_F)))
+        return out
+
+    def convert_wrf(self, fields, grid=None):
+        """WRF fields (dict ph/chem/rad/phy/moist, each [nfield][nj][nk][ni], host) -> the
+        context's cells (default grid: the reference's 48 x 20 x 48 domain and window)."""
+        g = WrfGrid()
+        if grid is None:
+            self.lib.radm2_wrf_grid_default(ctypes.byref(g))
+        else:
+            g = WrfGrid(*grid)
+        arrs = [np.ascontiguousarray(fields[k], dtype=np.float64) for k in ("ph", "chem", "rad", "phy", "moist")]
+        self._check(self.lib.radm2_convert_wrf(self.h, ctypes.byref(g), *[_dp(a) for a in arrs]))
+        self.ncell = g.wi * g.wk * g.wj
+
+    def get_inputs(self):
+        """The current per-cell inputs (reference layout)."""
+        n = self.ncell
+        out = {"VAR": np.empty((n, NVAR)), "FIX": np.empty((n, NFIX)), "TEMP": np.empty(n), "RC_N2O5": np.empty(n),
+               "JV": np.empty((n, NPH))}
+        self._check(self.lib.radm2_get_inputs(self.h, *[_dp(out[k]) for k in ("VAR", "FIX", "TEMP", "RC_N2O5", "JV")]))
         return out
 
     def opts(self):
