@@ -260,12 +260,15 @@ int radm2_mlp_synchronize(radm2_mlp *mlp);
 int radm2_mlp_set_h0_scale(radm2_mlp *mlp, float scale);
 /* Features of the context's current cell states, host out[ncell][84]. */
 int radm2_get_features(radm2_ctx *ctx, double dt, float *out);
-/* Seed the context from the network: per-cell starting steps (set_h0) and the
- * descending-predicted-cost cell order of the persistent schedule (set_order). */
+/* Seed the context from the network: per-cell starting steps (set_h0) and, for the
+ * persistent schedule, the cell order (set_order: 0 none, 1 cells by descending
+ * predicted cost, 2 chunks of 32 consecutive cells by their costliest cell, which keeps
+ * each warp's loads coalesced). */
 int radm2_seed_cells(radm2_ctx *ctx, radm2_mlp *mlp, double dt, int set_h0, int set_order);
 /* Attach a network to the context (NULL detaches): every following integration --
  * radm2_rosenbrock and each split of radm2_run_split -- is seeded from the current
- * state on the device first, inside the same CUDA graph for radm2_run_split. */
+ * state on the device first, inside the same CUDA graph for radm2_run_split.
+ * set_order as for radm2_seed_cells. */
 int radm2_attach_mlp(radm2_ctx *ctx, radm2_mlp *mlp, int set_order);
 
 /* Host-only consistency check of the library's kernel layouts (every thread's

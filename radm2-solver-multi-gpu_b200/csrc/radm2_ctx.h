@@ -50,15 +50,15 @@ struct radm2_ctx {
     float *seed_x = nullptr, *seed_y = nullptr;  // [seed_cap][84] features, [seed_cap][2] predictions
     bool use_h0 = true, use_order = true;  // whether the solver reads h0 / order when set
     radm2_mlp *mlp = nullptr;               // attached network: seeds every integration
-    bool mlp_order = false;
+    int mlp_order = 0;  // 0 none, 1 cells by predicted cost, 2 chunks of 32 cells by cost
 };
 
 namespace radm2 {
 // Drop a cached split graph (its baked-in arguments changed).
 void ctx_drop_graph(radm2_ctx *c);
 // Learned seeding (radm2_mlp.cu): buffers, then the stream-ordered kernels.
-int mlp_prepare_seed(radm2_ctx *c, radm2_mlp *m, bool order);
-cudaError_t mlp_enqueue_seed(radm2_ctx *c, radm2_mlp *m, double dt, bool order);
+int mlp_prepare_seed(radm2_ctx *c, radm2_mlp *m, int order);
+cudaError_t mlp_enqueue_seed(radm2_ctx *c, radm2_mlp *m, double dt, int order);
 unsigned int mlp_generation(const radm2_mlp *m);
 void mlp_detach(radm2_mlp *m);
 }  // namespace radm2

@@ -37,6 +37,13 @@ constexpr int S_ACT = S_WEND;                // activations: ROWS x KP bf16 (x, 
 constexpr int S_ACT2 = S_ACT + ROWS * KP;    // second activation buffer
 constexpr int S_TOTAL = S_ACT2 + ROWS * KP;  // bf16 elements
 constexpr int SMEM_BYTES = S_TOTAL * 2 + (W * 3 + NOUT) * 4 + NIN * 8;  // + biases + feature norm
+// The forward kernel runs 12 warps per CTA (192 rows per tile) over the one staged weight
+// image: 3x the warps of the training kernels, for latency hiding in the 1-CTA-per-SM
+// footprint (98 KB of weights + 8.7 KB of activations per warp).
+constexpr int FWD_WARPS = 12, FWD_ROWS = FWD_WARPS * 16;
+constexpr int FS_ACT = S_WEND, FS_ACT2 = FS_ACT + FWD_ROWS * KP, FS_TOTAL = FS_ACT2 + FWD_ROWS * KP;
+constexpr int FWD_SMEM_BYTES = FS_TOTAL * 2 + (W * 3 + NOUT) * 4 + NIN * 8;
+static_assert(FWD_SMEM_BYTES <= 227 * 1024, "forward kernel shared memory");
 
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
 {
@@ -119,24 +126,25 @@ __device__ void load_net(const Net &net, __nv_bfloat16 *sw, float *sb, float *sn
 
 // Forward over all layers for the CTA's rows.  Saves pre-activations z1..z3 (fp32) and the
 // outputs when the pointers are set (training).
-__global__ void __launch_bounds__(128) k_forward(Net net, int n, const float *__restrict__ x, float *__restrict__ y,
+__global__ void __launch_bounds__(FWD_WARPS * 32) k_forward(Net net, int n, const float *__restrict__ x,
+                                                            float *__restrict__ y,
                                                  float *__restrict__ z1, float *__restrict__ z2,
                                                  float *__restrict__ z3)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     __nv_bfloat16 *sw = reinterpret_cast<__nv_bfloat16 *>(smraw);
-    float *sb = reinterpret_cast<float *>(smraw + S_TOTAL * 2);
+    float *sb = reinterpret_cast<float *>(smraw + FS_TOTAL * 2);
     float *snorm = sb + 3 * W + NOUT;
     load_net(net, sw, sb, snorm);
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-    __nv_bfloat16 *act = sw + S_ACT + warp * 16 * KP;    // this warp's 16 rows
-    __nv_bfloat16 *act2 = sw + S_ACT2 + warp * 16 * KP;
-    const int ntiles = (n + ROWS - 1) / ROWS;
+    __nv_bfloat16 *act = sw + FS_ACT + warp * 16 * KP;  // this warp's 16 rows
+    __nv_bfloat16 *act2 = sw + FS_ACT2 + warp * 16 * KP;
+    const int ntiles = (n + FWD_ROWS - 1) / FWD_ROWS;
     // the weights are staged once per CTA; the CTA walks row tiles
 #pragma unroll 1
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int row0 = tile * ROWS + warp * 16;
+    const int row0 = tile * FWD_ROWS + warp * 16;
     __syncwarp();
     // normalised inputs -> bf16
     for (int i = lane; i < 16 * NIN; i += 32) {
@@ -434,6 +442,32 @@ __global__ void k_seed(int n, const float *__restrict__ y, float m0, float s0, f
     idx[c] = c;
 }
 
+// Cost order by chunks of 32 consecutive cells: a chunk's key is its costliest cell's
+// (the smallest flipped key); a partial last chunk sorts last.  Keeping 32 consecutive
+// cells together keeps the solver's loads of a warp's cells coalesced.
+constexpr int ORDER_CHUNK = 32;
+
+__global__ void k_chunk_keys(int n, const unsigned int *__restrict__ key, unsigned int *__restrict__ ckey,
+                             int *__restrict__ cidx)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nq = (n + ORDER_CHUNK - 1) / ORDER_CHUNK;
+    if (q >= nq) return;
+    const int lo = q * ORDER_CHUNK, hi = min(n, lo + ORDER_CHUNK);
+    unsigned int k = 0xFFFFFFFFu;
+    if (hi - lo == ORDER_CHUNK)
+        for (int c = lo; c < hi; c++) k = min(k, key[c]);
+    ckey[q] = k;
+    cidx[q] = q;
+}
+
+__global__ void k_expand_chunks(int n, const int *__restrict__ chunk, int *__restrict__ order)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    order[p] = chunk[p / ORDER_CHUNK] * ORDER_CHUNK + p % ORDER_CHUNK;
+}
+
 }  // namespace mlp
 }  // namespace radm2
 
@@ -502,7 +536,7 @@ cudaError_t set_kernel_attributes()
 {
     static bool done = false;
     if (done) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(k_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    cudaError_t e = cudaFuncSetAttribute(k_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, FWD_SMEM_BYTES);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
     done = e == cudaSuccess;
     return e;
@@ -513,10 +547,10 @@ cudaError_t forward(radm2_mlp *m, int n, const float *dx, float *dy, bool keep, 
     cudaError_t e0 = set_kernel_attributes();
     if (e0 != cudaSuccess) return e0;
     const size_t zs = (size_t)m->zcap * W;
-    const int ntiles = (n + ROWS - 1) / ROWS;
+    const int ntiles = (n + FWD_ROWS - 1) / FWD_ROWS;
     const int grid = ntiles < m->nsm ? ntiles : m->nsm;  // one CTA per SM walks the row tiles
     (void)cudaGetLastError();
-    k_forward<<<grid, 128, SMEM_BYTES, st>>>(net_of(m), n, dx, dy, keep ? m->z : nullptr,
+    k_forward<<<grid, FWD_WARPS * 32, FWD_SMEM_BYTES, st>>>(net_of(m), n, dx, dy, keep ? m->z : nullptr,
                                                                  keep ? m->z + zs : nullptr,
                                                                  keep ? m->z + 2 * zs : nullptr);
     return cudaGetLastError();
@@ -538,7 +572,7 @@ cudaError_t backward(radm2_mlp *m, int n, const float *dx, const float *dt)
 // the order with its sort workspace when asked).  The rows belong to the context, so a
 // captured graph never reads buffers that the network may reallocate; nothing is
 // allocated again while the cell count stays the same.
-int radm2::mlp_prepare_seed(radm2_ctx *c, radm2_mlp *m, bool order)
+int radm2::mlp_prepare_seed(radm2_ctx *c, radm2_mlp *m, int order)
 {
     (void)m;
     const int n = c->ncell;
@@ -555,7 +589,8 @@ int radm2::mlp_prepare_seed(radm2_ctx *c, radm2_mlp *m, bool order)
         c->seed_tmp_bytes = 0;
         c->seed_cap = 0;
         e = cudaMalloc((void **)&c->seed_keys, sizeof(unsigned int) * (size_t)n * 2);
-        if (e == cudaSuccess) e = cudaMalloc((void **)&c->seed_idx, sizeof(int) * (size_t)n);
+        // per-cell indices, then room for chunk indices in and out of the chunk sort
+        if (e == cudaSuccess) e = cudaMalloc((void **)&c->seed_idx, sizeof(int) * ((size_t)n + 2 * (size_t)(n / 32 + 1)));
         if (e == cudaSuccess) e = cudaMalloc((void **)&c->seed_x, sizeof(float) * (size_t)n * NFEAT);
         if (e == cudaSuccess) e = cudaMalloc((void **)&c->seed_y, sizeof(float) * (size_t)n * NY);
         if (e == cudaSuccess) c->seed_cap = n;
@@ -577,7 +612,7 @@ void radm2::mlp_detach(radm2_mlp *m) { m->attached--; }
 
 // Stream-ordered seeding on the context's stream (capturable): features -> network ->
 // per-cell h0 (and the descending-cost order when asked).
-cudaError_t radm2::mlp_enqueue_seed(radm2_ctx *c, radm2_mlp *m, double dt, bool order)
+cudaError_t radm2::mlp_enqueue_seed(radm2_ctx *c, radm2_mlp *m, double dt, int order)
 {
     const int n = c->ncell;
     (void)cudaGetLastError();
@@ -589,10 +624,23 @@ cudaError_t radm2::mlp_enqueue_seed(radm2_ctx *c, radm2_mlp *m, double dt, bool 
                                                    m->h0_scale, c->h0, c->seed_keys, c->seed_idx);
         e = cudaGetLastError();
     }
-    if (e == cudaSuccess && order) {
+    if (e == cudaSuccess && order == 1) {
         size_t tb = c->seed_tmp_bytes;
         e = cub::DeviceRadixSort::SortPairs(c->seed_tmp, tb, c->seed_keys, c->seed_keys + n, c->seed_idx, c->order, n,
                                             0, 32, c->st);
+    } else if (e == cudaSuccess && order == 2) {
+        const int nq = (n + ORDER_CHUNK - 1) / ORDER_CHUNK;
+        unsigned int *ckey = c->seed_keys + n;  // chunk keys in the second half, sorted into the first
+        int *cin = c->seed_idx + n, *cout = c->seed_idx + n + nq;
+        k_chunk_keys<<<(nq + 127) / 128, 128, 0, c->st>>>(n, c->seed_keys, ckey, cin);
+        e = cudaGetLastError();
+        size_t tb = c->seed_tmp_bytes;
+        if (e == cudaSuccess)
+            e = cub::DeviceRadixSort::SortPairs(c->seed_tmp, tb, ckey, c->seed_keys, cin, cout, nq, 0, 32, c->st);
+        if (e == cudaSuccess) {
+            k_expand_chunks<<<(n + 127) / 128, 128, 0, c->st>>>(n, cout, c->order);
+            e = cudaGetLastError();
+        }
     }
     return e;
 }
@@ -796,9 +844,10 @@ int radm2_seed_cells(radm2_ctx *c, radm2_mlp *m, double dt, int set_h0, int set_
     if (!c || !m || !(dt > 0.0)) return RADM2_E_ARG;
     if (!c->var) return RADM2_E_STATE;
     cudaSetDevice(c->o.device);
-    int rc = radm2::mlp_prepare_seed(c, m, set_order != 0);
+    if (set_order < 0 || set_order > 2) return RADM2_E_ARG;
+    int rc = radm2::mlp_prepare_seed(c, m, set_order);
     if (rc) return rc;
-    if (radm2::mlp_enqueue_seed(c, m, dt, set_order != 0) != cudaSuccess || cudaStreamSynchronize(c->st) != cudaSuccess) {
+    if (radm2::mlp_enqueue_seed(c, m, dt, set_order) != cudaSuccess || cudaStreamSynchronize(c->st) != cudaSuccess) {
         c->err = "radm2_seed_cells: CUDA error";
         return RADM2_E_CUDA;
     }
@@ -812,18 +861,19 @@ int radm2_attach_mlp(radm2_ctx *c, radm2_mlp *m, int set_order)
     if (!c) return RADM2_E_ARG;
     if (!c->var) return RADM2_E_STATE;
     cudaSetDevice(c->o.device);
+    if (set_order < 0 || set_order > 2) return RADM2_E_ARG;
     if (m && m->device != c->o.device) {
         c->err = "radm2_attach_mlp: network and context are on different devices";
         return RADM2_E_ARG;
     }
     if (m) {
-        int rc = radm2::mlp_prepare_seed(c, m, set_order != 0);
+        int rc = radm2::mlp_prepare_seed(c, m, set_order);
         if (rc) return rc;
     }
     radm2::ctx_drop_graph(c);
     if (c->mlp) c->mlp->attached--;
     c->mlp = m;
-    c->mlp_order = m && set_order;
+    c->mlp_order = m ? set_order : 0;
     if (!m) return RADM2_OK;
     m->attached++;
     // the network's stream may still be writing its weights (training)

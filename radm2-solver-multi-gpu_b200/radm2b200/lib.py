@@ -362,12 +362,15 @@ class Solver:
         return [{k: getattr(tab[i], k) for k, _ in TuneEntry._fields_} for i in range(min(n.value, 64))]
 
     def attach_mlp(self, mlp, order=False):
-        """Seed every following integration from the network (None detaches)."""
-        self._check(self.lib.radm2_attach_mlp(self.h, mlp.h if mlp is not None else None, 1 if order else 0))
+        """Seed every following integration from the network (None detaches); order: False/0
+        none, True/1 cells by predicted cost, 2 chunks of 32 cells by cost."""
+        mode = 1 if order is True else int(order or 0)  # 0 none, 1 cells, 2 chunks of 32 cells
+        self._check(self.lib.radm2_attach_mlp(self.h, mlp.h if mlp is not None else None, mode))
         self._mlp = mlp  # keep the network alive while attached
 
     def seed_cells(self, mlp, dt, h0=True, order=True):
-        self._check(self.lib.radm2_seed_cells(self.h, mlp.h, dt, 1 if h0 else 0, 1 if order else 0))
+        mode = 1 if order is True else int(order or 0)
+        self._check(self.lib.radm2_seed_cells(self.h, mlp.h, dt, 1 if h0 else 0, mode))
 
     # ---- mechanism kernels
     def fun(self, V, FIX, RCT):

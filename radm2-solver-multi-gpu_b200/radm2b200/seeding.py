@@ -10,6 +10,8 @@ back to the default Hstart) and, optionally, order cells by descending predicted
 for the persistent schedule.  Attached to a solver (Solver.attach_mlp), the seeding
 kernels run in front of every split inside the split loop's CUDA graph.
 """
+import os
+
 import numpy as np
 
 from . import inputs
@@ -102,6 +104,11 @@ def train_default(device=0, dt=600.0, log=None):
     return net, {"pairs": int(X.shape[0]), "loss": float(hist[-1]), "epochs": TRAIN_EPOCHS,
                  "trace_cells": TRAIN_CELLS, "trace_splits": TRAIN_SPLITS, "trace_seed": TRAIN_SEED,
                  "h0_safety": H0_SAFETY}
+
+
+# A network trained by train_default (regenerate: python bench.py --save-weights PATH, or
+# save_net(train_default()[0], PATH)), shipped for seeding without training first.
+DEFAULT_NET = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "seed_net_mixed.npz")
 
 
 def save_net(net, path, h0_scale=H0_SAFETY):

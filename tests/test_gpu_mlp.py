@@ -119,3 +119,22 @@ def test_attached_seeding_in_graph_matches_host_driven():
         # a network still attached cannot be destroyed
         assert radm2b200.lib.load().radm2_mlp_destroy(net.h) == radm2b200.lib.RADM2_E_STATE
         s.attach_mlp(None)
+
+
+@pytest.mark.parametrize("order", [1, 2])
+def test_cost_order_changes_schedule_not_results(order):
+    """Ordering cells (one by one, or in chunks of 32) by predicted cost changes which lane
+    takes which cell, not any cell's arithmetic: results equal the unordered run's."""
+    cells = inputs.make_cells(3000, 13, "mixed")  # not a multiple of 32: a partial chunk
+    net = seeding.load_net(seeding.DEFAULT_NET)
+    out = []
+    for o in (0, order):
+        with radm2b200.Solver(schedule=radm2b200.SCHED_PERSISTENT) as s:
+            s.set_cells(cells)
+            s.attach_mlp(net, order=o)
+            ipar, rpar = radm2b200.default_params()
+            assert s.run_split(2, 600.0, seeding.ATOL, seeding.RTOL, rpar, ipar) == 1
+            out.append((s.get_state(), int(ipar[13]), int(ipar[14])))
+            s.attach_mlp(None)
+    assert out[0][1:] == out[1][1:]
+    assert np.array_equal(out[0][0], out[1][0])
