@@ -427,6 +427,8 @@ def main():
         if main_arm["tuned"] is not None:
             sched_used = "persistent" if main_arm["tuned"]["chosen"]["schedule"] else "static"
         key = "%s-%s" % (args.precision, sched_used)
+        if key + "-" + wl in tr:  # a capture of this workload family, if there is one
+            key = key + "-" + wl
         if key in tr:
             # DRAM bytes per step attempt from one ncu capture (small case), scaled to the
             # attempts of an average launch here: traffic grows with attempts, not cells
