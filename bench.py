@@ -76,6 +76,8 @@ def parse():
     ap.add_argument("--weights", default="", help="seeding network stored by --save-weights (skip training)")
     ap.add_argument("--save-weights", default="")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain comparison arm")
+    ap.add_argument("--ref-step-seconds", type=float, default=8.0,
+                    help="reference arm: size each step's CPU sample to about this long")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -188,8 +190,8 @@ def run_reference(args):
     probe_cells = inputs.make_cells(min(ncell, 1024), seed, wl, night)
     _, tp = oracle_sample(probe_cells, len(probe_cells["TEMP"]), 1, dt, RTOL, nthreads)
     per_cell = tp / len(probe_cells["TEMP"])
-    # each step ~8 s of work on this host: the first n cells of the workload
-    n = int(min(ncell, max(1024, 8.0 / max(per_cell, 1e-9))))
+    # each step ~ref_step_seconds of work on this host: the first n cells of the workload
+    n = int(min(ncell, max(256, args.ref_step_seconds / max(per_cell, 1e-9))))
     cells = inputs.make_cells(n, seed, wl, night)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
