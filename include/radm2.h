@@ -191,6 +191,20 @@ int radm2_fma_peak(int device, double *fp64_tflops, double *fp32_tflops);
 /* Number of cells and device bytes held by the context. */
 int radm2_get_ncell(const radm2_ctx *ctx);
 
+/* One integration straight from host arrays in the reference's per-cell layout -- the
+ * whole radm2_set_inputs + radm2_rosenbrock + radm2_get_state sequence (mgpu.cu:648-680,
+ * 921-947, 3664-3848) in one call -- with the transfers overlapped with the solve: the
+ * batch is cut into nchunk consecutive chunks (at least 1,024 cells each), chunk k's
+ * inputs upload while chunk k-1 integrates and chunk k-2's states download.  VAR is read
+ * and overwritten with the result; RC_N2O5 may be NULL (reference formula).  Rate
+ * constants and, with a network attached, the seeded starting steps are formed per chunk;
+ * a cost order is not applied.  Host arrays should be page-locked (cudaHostRegister /
+ * cudaMallocHost): pageable memory is correct but serialises the copies.  Returns IERR and
+ * fills IPAR/RPAR as radm2_rosenbrock. */
+int radm2_rosenbrock_host(radm2_ctx *ctx, int ncell, double *VAR, const double *FIX, const double *TEMP,
+                          const double *RC_N2O5, const double *JV, double Tstart, double Tend, const double *AbsTol,
+                          const double *RelTol, double *RPAR, int *IPAR, int nchunk);
+
 /* WRF -> KPP conversion, replacing dev_convert + convertWRFChemData (mgpu.cu:513-706).
  * WRF fields are field-major with i fastest, field[f][nj][nk][ni]; the window
  * [i0, i0+wi) x [k0, k0+wk) x [j0, j0+wj) becomes the context's cells, cell

@@ -482,6 +482,9 @@ int radm2_destroy(radm2_ctx *c)
     if (c->d_res) cudaFree(c->d_res);
     if (c->h_res) cudaFreeHost(c->h_res);
     if (c->queue) cudaFree(c->queue);
+    for (cudaEvent_t e : c->pipe_ev) cudaEventDestroy(e);
+    if (c->st_up) cudaStreamDestroy(c->st_up);
+    if (c->st_down) cudaStreamDestroy(c->st_down);
     if (c->own) cudaStreamDestroy(c->own);
     delete c;
     return RADM2_OK;
@@ -657,6 +660,117 @@ int radm2_rosenbrock(radm2_ctx *c, double Tstart, double Tend, const double *Abs
     if ((rc = enqueue_integration(c, p, 0, bs, grid))) return rc;
     CK(cudaMemcpyAsync(c->h_res, c->d_res, sizeof(RunResult), cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
+    return finish(c, 1, autonomous, RPAR, IPAR, p.direction);
+}
+
+// Host-buffer integration with the transfers hidden behind the solve: the batch is cut into
+// nchunk consecutive chunks.  Chunk k's inputs go up (copy stream, then a transpose to the
+// struct-of-arrays arrays) while chunk k-1 integrates (rate constants, optional seeding,
+// solver, statistics on the context's stream) and chunk k-2's states come back (transpose
+// and copy on a second copy stream).  Events order each chunk's three steps.
+int radm2_rosenbrock_host(radm2_ctx *c, int ncell, double *VAR, const double *FIX, const double *TEMP,
+                          const double *RC_N2O5, const double *JV, double Tstart, double Tend, const double *AbsTol,
+                          const double *RelTol, double *RPAR, int *IPAR, int nchunk)
+{
+    if (!valid_ctx(c) || ncell <= 0 || !VAR || !FIX || !TEMP || !JV || !AbsTol || !RelTol || !RPAR || !IPAR)
+        return RADM2_E_ARG;
+    CK(cudaSetDevice(c->o.device));
+    SolveParams p;
+    int autonomous = 1;
+    int ierr = parse_params(Tstart, Tend, AbsTol, RelTol, RPAR, IPAR, c->o.float_coeffs, &p, &autonomous);
+    if (ierr != 1) return ierr;
+    int rc = ensure_cells(c, ncell);
+    if (rc) return rc;
+    c->have_rcn = RC_N2O5 != nullptr;
+    c->rconst_valid = false;  // recomputed per chunk below
+    nchunk = std::max(1, std::min(nchunk, (ncell + 1023) / 1024));
+    int bs, grid;
+    size_t sbytes;
+    if ((rc = launch_geometry(c, &bs, &grid, &sbytes))) return rc;
+    if ((rc = ensure_scratch(c, sbytes))) return rc;
+    if ((rc = ensure_results(c, nchunk))) return rc;
+    if (c->mlp && (rc = mlp_prepare_seed(c, c->mlp, 0))) return rc;
+    // staging: inputs in the reference layout (VAR, FIX, TEMP, RC_N2O5, JV), then the states
+    const int win = NVAR + NFIX + 2 + NPH;
+    const size_t n = (size_t)ncell;
+    if ((rc = ensure_stage(c, sizeof(double) * n * (win + NVAR)))) return rc;
+    double *sv = c->stage, *sf = sv + n * NVAR, *st_ = sf + n * NFIX, *sr = st_ + n, *sj = sr + n, *so = sj + n * NPH;
+    if (!c->st_up) CK(cudaStreamCreateWithFlags(&c->st_up, cudaStreamNonBlocking));
+    if (!c->st_down) CK(cudaStreamCreateWithFlags(&c->st_down, cudaStreamNonBlocking));
+    while ((int)c->pipe_ev.size() < 2 * nchunk) {
+        cudaEvent_t e;
+        CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        c->pipe_ev.push_back(e);
+    }
+    const bool order_was = c->use_order;
+    c->use_order = false;  // a chunk's cells are integrated in index order
+    const double dt = std::fabs(p.Tend - p.Tstart);
+    for (int k = 0; k < nchunk; k++) {
+        const int lo = (int)(n * k / nchunk), hi = (int)(n * (k + 1) / nchunk), m = hi - lo;
+        const size_t l = (size_t)lo;
+        // up: copies of this chunk's rows, then the transposes into the cell arrays
+        CK(cudaMemcpyAsync(sv + l * NVAR, VAR + l * NVAR, sizeof(double) * m * NVAR, cudaMemcpyHostToDevice, c->st_up));
+        CK(cudaMemcpyAsync(sf + l * NFIX, FIX + l * NFIX, sizeof(double) * m * NFIX, cudaMemcpyHostToDevice, c->st_up));
+        CK(cudaMemcpyAsync(st_ + l, TEMP + l, sizeof(double) * m, cudaMemcpyHostToDevice, c->st_up));
+        if (RC_N2O5) CK(cudaMemcpyAsync(sr + l, RC_N2O5 + l, sizeof(double) * m, cudaMemcpyHostToDevice, c->st_up));
+        CK(cudaMemcpyAsync(sj + l * NPH, JV + l * NPH, sizeof(double) * m * NPH, cudaMemcpyHostToDevice, c->st_up));
+        CK(launch_aos_to_soa(m, NVAR, c->ld, sv + l * NVAR, c->var + lo, c->st_up));
+        CK(launch_aos_to_soa(m, NFIX, c->ld, sf + l * NFIX, c->fix + lo, c->st_up));
+        CK(cudaMemcpyAsync(c->temp + lo, st_ + l, sizeof(double) * m, cudaMemcpyDeviceToDevice, c->st_up));
+        if (RC_N2O5) CK(cudaMemcpyAsync(c->rcn + lo, sr + l, sizeof(double) * m, cudaMemcpyDeviceToDevice, c->st_up));
+        CK(launch_aos_to_soa(m, NPH, c->ld, sj + l * NPH, c->jv + lo, c->st_up));
+        CK(cudaEventRecord(c->pipe_ev[2 * k], c->st_up));
+        // integrate the chunk
+        CK(cudaStreamWaitEvent(c->st, c->pipe_ev[2 * k], 0));
+        CK(launch_rconst(m, c->ld, c->jv + lo, c->temp + lo, c->fix + lo, RC_N2O5 ? c->rcn + lo : nullptr,
+                         c->rconst + lo, c->st));
+        if (c->mlp) CK(mlp_enqueue_seed(c, c->mlp, dt, 0, lo, m));
+        CK(cudaMemsetAsync(c->queue + k, 0, sizeof(int), c->st));
+        SolveArgs a = make_args(c, p, c->queue + k);
+        a.ncell = m;
+        a.var += lo;
+        a.fix += lo;
+        a.rconst += lo;
+        if (a.h0) a.h0 += lo;
+        a.status += lo;
+        a.nacc += lo;
+        a.nrej += lo;
+        a.hfirst += lo;
+        a.hexit += lo;
+        a.texit += lo;
+        int kg = grid;
+        if (c->o.schedule == RADM2_SCHED_PERSISTENT) kg = std::min(grid, (m + bs - 1) / bs);
+        else kg = (m + bs - 1) / bs;
+        CK(launch_solver(c, a, bs, std::max(kg, 1)));
+        CK(launch_reduce(m, c->status + lo, c->nacc + lo, c->nrej + lo, c->texit + lo, c->hexit + lo, c->partials,
+                         c->d_res + k, c->st));
+        CK(cudaEventRecord(c->pipe_ev[2 * k + 1], c->st));
+        // down: this chunk's states
+        CK(cudaStreamWaitEvent(c->st_down, c->pipe_ev[2 * k + 1], 0));
+        CK(launch_soa_to_aos(m, NVAR, c->ld, c->var + lo, so + l * NVAR, c->st_down));
+        CK(cudaMemcpyAsync(VAR + l * NVAR, so + l * NVAR, sizeof(double) * m * NVAR, cudaMemcpyDeviceToHost,
+                           c->st_down));
+    }
+    c->use_order = order_was;
+    CK(cudaMemcpyAsync(c->h_res, c->d_res, sizeof(RunResult) * nchunk, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    CK(cudaStreamSynchronize(c->st_down));
+    CK(cudaStreamSynchronize(c->st_up));
+    // one result over all chunks: counters summed, exit times and steps at their extremes
+    RunResult tot = c->h_res[0];
+    for (int k = 1; k < nchunk; k++) {
+        const RunResult &r = c->h_res[k];
+        tot.nacc += r.nacc;
+        tot.nrej += r.nrej;
+        tot.nfail += r.nfail;
+        tot.worst = std::min(tot.worst, r.worst);
+        tot.max_att = std::max(tot.max_att, r.max_att);
+        tot.tmin = std::min(tot.tmin, r.tmin);
+        tot.tmax = std::max(tot.tmax, r.tmax);
+        tot.hmin = std::min(tot.hmin, r.hmin);
+    }
+    c->h_res[0] = tot;
+    c->rconst_valid = true;
     return finish(c, 1, autonomous, RPAR, IPAR, p.direction);
 }
 

@@ -12,6 +12,8 @@ struct radm2_ctx {
     int nsm = 0;
     cudaStream_t own = nullptr;
     cudaStream_t st = nullptr;
+    cudaStream_t st_up = nullptr, st_down = nullptr;  // copy streams of the pipelined host path
+    std::vector<cudaEvent_t> pipe_ev;                 // per chunk: inputs up, chunk integrated
     int ncell = 0, ld = 0;
     double *var = nullptr, *fix = nullptr, *temp = nullptr, *rcn = nullptr, *jv = nullptr, *rconst = nullptr;
     bool have_rcn = false;
@@ -58,7 +60,7 @@ namespace radm2 {
 void ctx_drop_graph(radm2_ctx *c);
 // Learned seeding (radm2_mlp.cu): buffers, then the stream-ordered kernels.
 int mlp_prepare_seed(radm2_ctx *c, radm2_mlp *m, int order);
-cudaError_t mlp_enqueue_seed(radm2_ctx *c, radm2_mlp *m, double dt, int order);
+cudaError_t mlp_enqueue_seed(radm2_ctx *c, radm2_mlp *m, double dt, int order, int lo = 0, int count = -1);
 unsigned int mlp_generation(const radm2_mlp *m);
 void mlp_detach(radm2_mlp *m);
 }  // namespace radm2

@@ -612,16 +612,19 @@ void radm2::mlp_detach(radm2_mlp *m) { m->attached--; }
 
 // Stream-ordered seeding on the context's stream (capturable): features -> network ->
 // per-cell h0 (and the descending-cost order when asked).
-cudaError_t radm2::mlp_enqueue_seed(radm2_ctx *c, radm2_mlp *m, double dt, int order)
+cudaError_t radm2::mlp_enqueue_seed(radm2_ctx *c, radm2_mlp *m, double dt, int order, int lo, int count)
 {
-    const int n = c->ncell;
+    // cells [lo, lo + count) (count < 0: all); a sub-range gets h0 only, no order
+    const int n = count < 0 ? c->ncell : count;
+    if (count >= 0) order = 0;
     (void)cudaGetLastError();
-    k_features<<<(n + 127) / 128, 128, 0, c->st>>>(n, c->ld, c->var, c->fix, c->temp, c->jv, (float)dt, c->seed_x);
+    k_features<<<(n + 127) / 128, 128, 0, c->st>>>(n, c->ld, c->var + lo, c->fix + lo, c->temp + lo, c->jv + lo,
+                                                   (float)dt, c->seed_x);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = forward(m, n, c->seed_x, c->seed_y, false, c->st);
     if (e == cudaSuccess) {
         k_seed<<<(n + 127) / 128, 128, 0, c->st>>>(n, c->seed_y, m->ymean[0], m->ystd[0], m->ymean[1], m->ystd[1],
-                                                   m->h0_scale, c->h0, c->seed_keys, c->seed_idx);
+                                                   m->h0_scale, c->h0 + lo, c->seed_keys, c->seed_idx);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess && order == 1) {

@@ -99,6 +99,9 @@ SIGNATURES = {
                                         ctypes.c_int]),
     "radm2_attach_mlp": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]),
     "radm2_get_ncell": (ctypes.c_int, [ctypes.c_void_p]),
+    "radm2_rosenbrock_host": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _D, _D, _D, _D, _D, ctypes.c_double,
+                                             ctypes.c_double, _D, _D, _D, ctypes.POINTER(ctypes.c_int),
+                                             ctypes.c_int]),
     "radm2_get_inputs": (ctypes.c_int, [ctypes.c_void_p, _D, _D, _D, _D, _D]),
     "radm2_wrf_grid_default": (ctypes.c_int, [ctypes.POINTER(WrfGrid)]),
     "radm2_convert_wrf": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(WrfGrid), _D, _D, _D, _D, _D]),
@@ -341,6 +344,21 @@ class Solver:
                "JV": np.empty((n, NPH))}
         self._check(self.lib.radm2_get_inputs(self.h, *[_dp(out[k]) for k in ("VAR", "FIX", "TEMP", "RC_N2O5", "JV")]))
         return out
+
+    def rosenbrock_host(self, VAR, FIX, TEMP, RC_N2O5, JV, tstart, tend, atol, rtol, rpar, ipar, nchunk=8):
+        """Integrate host arrays (reference layout) with copies overlapped with the solve;
+        VAR (float64, C-contiguous) is overwritten with the result.  Returns IERR."""
+        n = VAR.shape[0]
+        if VAR.dtype != np.float64 or not VAR.flags.c_contiguous or VAR.shape[1] != NVAR:
+            raise ValueError("VAR must be a C-contiguous float64 [n][59] array (updated in place)")
+        FIX, TEMP, JV = _c64(FIX, (n, NFIX)), _c64(TEMP, (n,)), _c64(JV, (n, NPH))
+        rcn = None if RC_N2O5 is None else _c64(RC_N2O5, (n,))
+        atol, rtol = _c64(atol), _c64(rtol)
+        ierr = self.lib.radm2_rosenbrock_host(self.h, n, _dp(VAR), _dp(FIX), _dp(TEMP),
+                                              _dp(rcn) if rcn is not None else None, _dp(JV), tstart, tend,
+                                              _dp(atol), _dp(rtol), _dp(rpar), _ip(ipar), nchunk)
+        self.ncell = n
+        return ierr
 
     def opts(self):
         """The options in force (the autotuner rewrites schedule / block shape / placement)."""

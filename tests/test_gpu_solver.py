@@ -234,3 +234,48 @@ def test_autotune_picks_fastest_and_keeps_results():
         assert s.run_split(1, 600.0, atol, rtol, rpar, ipar) == 1
         assert int(ipar[13]) == acc_before
         assert rel_err(s.get_state(), y_before).max() <= 1e-13
+
+
+@pytest.mark.parametrize("nchunk", [1, 5])
+def test_pipelined_host_integration_matches_separate_calls(nchunk):
+    """radm2_rosenbrock_host (chunked, copies overlapped with the solve) gives exactly what
+    set_inputs + rosenbrock + get_state give, counters included."""
+    cells = inputs.make_cells(20000, 9, "mixed")
+    atol, rtol = np.ones(59), np.full(59, 1e-3)
+    with radm2b200.Solver(schedule=radm2b200.SCHED_PERSISTENT) as s:
+        s.set_cells(cells)
+        ipar0, rpar0 = radm2b200.default_params(hstart=6.0)
+        assert s.rosenbrock(0.0, 600.0, atol, rtol, rpar0, ipar0) == 1
+        y0 = s.get_state()
+    with radm2b200.Solver(schedule=radm2b200.SCHED_PERSISTENT) as s:
+        y = np.ascontiguousarray(cells["VAR"]).copy()
+        ipar, rpar = radm2b200.default_params(hstart=6.0)
+        ierr = s.rosenbrock_host(y, cells["FIX"], cells["TEMP"], cells["RC_N2O5"], cells["JV"], 0.0, 600.0, atol,
+                                 rtol, rpar, ipar, nchunk=nchunk)
+        assert ierr == 1
+    assert np.array_equal(y, y0)
+    assert list(ipar[10:17]) == list(ipar0[10:17])
+    assert rpar[10] == rpar0[10] and rpar[11] == rpar0[11]
+
+
+def test_pipelined_host_integration_with_seeding():
+    from radm2b200 import seeding
+    cells = inputs.make_cells(12000, 10, "mixed")
+    net = seeding.load_net(seeding.DEFAULT_NET)
+    outs = []
+    for chunked in (False, True):
+        with radm2b200.Solver(schedule=radm2b200.SCHED_PERSISTENT) as s:
+            s.set_cells(cells)
+            s.attach_mlp(net)
+            ipar, rpar = radm2b200.default_params()
+            if chunked:
+                y = np.ascontiguousarray(cells["VAR"]).copy()
+                assert s.rosenbrock_host(y, cells["FIX"], cells["TEMP"], cells["RC_N2O5"], cells["JV"], 0.0, 600.0,
+                                         seeding.ATOL, seeding.RTOL, rpar, ipar, nchunk=4) == 1
+            else:
+                assert s.rosenbrock(0.0, 600.0, seeding.ATOL, seeding.RTOL, rpar, ipar) == 1
+                y = s.get_state()
+            s.attach_mlp(None)
+        outs.append((y, int(ipar[13]), int(ipar[14])))
+    assert outs[0][1:] == outs[1][1:]
+    assert np.array_equal(outs[0][0], outs[1][0])
