@@ -226,6 +226,18 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def per_species_errors(y, ref):
+    """{species: [max, median]} relative error over cells where the species is above atol."""
+    from radm2b200 import inputs
+    out = {}
+    for i, name in enumerate(inputs.SPECIES):
+        m = np.abs(ref[:, i]) > ATOL
+        if m.any():
+            e = np.abs(y[m, i] - ref[m, i]) / np.abs(ref[m, i])
+            out[name] = [float("%.3g" % e.max()), float("%.3g" % np.median(e))]
+    return out
+
+
 def rel_errors(y, ref):
     """Relative errors of y against ref on entries above atol, and on entries where the
     relative tolerance governs the error control (|ref| >= atol / rtol)."""
@@ -421,7 +433,8 @@ def main():
         accuracy = {"reference": "FP64 rtol 1e-8 (GPU plain path; %d of its cells re-run by the CPU oracle: "
                                  "max rel diff %.1e)" % (nchk, chk),
                     "cells": na, "tight_seconds": tight_s,
-                    args.method: rel_errors(y_main[idx], y_tight)}
+                    args.method: rel_errors(y_main[idx], y_tight),
+                    "per_species_" + args.method: per_species_errors(y_main[idx], y_tight)}
         if plain is not None:
             accuracy["plain"] = rel_errors(y_plain[idx], y_tight)
             a, b = accuracy[args.method]["above_atol"], accuracy["plain"]["above_atol"]
