@@ -190,13 +190,14 @@ int radm2_fma_peak(int device, double *fp64_tflops, double *fp32_tflops);
 
 /* Number of cells and device bytes held by the context. */
 int radm2_get_ncell(const radm2_ctx *ctx);
+size_t radm2_device_bytes(const radm2_ctx *ctx);
 
 /* One integration straight from host arrays in the reference's per-cell layout -- the
  * whole radm2_set_inputs + radm2_rosenbrock + radm2_get_state sequence (mgpu.cu:648-680,
  * 921-947, 3664-3848) in one call -- with the transfers overlapped with the solve: the
  * batch is cut into nchunk consecutive chunks (at least 1,024 cells each), chunk k's
  * inputs upload while chunk k-1 integrates and chunk k-2's states download.  VAR is read
- * and overwritten with the result; RC_N2O5 may be NULL (reference formula).  Rate
+ * and overwritten with the result; RC_N2O5 may be NULL (zero, as for radm2_set_inputs).  Rate
  * constants and, with a network attached, the seeded starting steps are formed per chunk;
  * a cost order is not applied.  Host arrays should be page-locked (cudaHostRegister /
  * cudaMallocHost): pageable memory is correct but serialises the copies.  Returns IERR and
@@ -242,7 +243,6 @@ typedef struct radm2_tune_entry {
 } radm2_tune_entry;
 int radm2_autotune(radm2_ctx *ctx, double dt, const double *AbsTol, const double *RelTol, const double *RPAR,
                    const int *IPAR, int sample_cells, radm2_tune_entry *table, int table_len, int *n_entries);
-size_t radm2_device_bytes(const radm2_ctx *ctx);
 
 /*
  * Learned step seeding.  A small network (84 state features -> 3 x 128 GELU -> 2, BF16
