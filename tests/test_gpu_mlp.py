@@ -138,3 +138,24 @@ def test_cost_order_changes_schedule_not_results(order):
             s.attach_mlp(None)
     assert out[0][1:] == out[1][1:]
     assert np.array_equal(out[0][0], out[1][0])
+
+
+def test_nonfinite_predictions_fall_back_to_default_step():
+    """A network whose outputs are not finite seeds nothing: every cell starts from the
+    default Hstart, so the result equals the unseeded integration."""
+    cells = inputs.make_cells(2048, 14, "mixed")
+    bad = radm2b200.Mlp(seed=1)
+    bad.set_params(np.full(bad.nparams, np.nan, dtype=np.float32))
+    bad.set_norm(np.zeros(84), np.ones(84), np.zeros(2), np.ones(2))
+    outs = []
+    for net in (None, bad):
+        with radm2b200.Solver(schedule=radm2b200.SCHED_PERSISTENT) as s:
+            s.set_cells(cells)
+            if net is not None:
+                s.attach_mlp(net)
+            ipar, rpar = radm2b200.default_params()
+            assert s.run_split(1, 600.0, seeding.ATOL, seeding.RTOL, rpar, ipar) == 1
+            outs.append((s.get_state(), int(ipar[13]), int(ipar[14])))
+            s.attach_mlp(None)
+    assert outs[0][1:] == outs[1][1:]
+    assert np.array_equal(outs[0][0], outs[1][0])

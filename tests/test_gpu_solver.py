@@ -279,3 +279,25 @@ def test_pipelined_host_integration_with_seeding():
         outs.append((y, int(ipar[13]), int(ipar[14])))
     assert outs[0][1:] == outs[1][1:]
     assert np.array_equal(outs[0][0], outs[1][0])
+
+
+@pytest.mark.parametrize("n", [1, 31, 33])
+def test_tiny_and_odd_batches_match_oracle(n):
+    """Batches smaller than a warp or just over it (padding of the leading dimension):
+    static and persistent schedules agree with each other and with the oracle."""
+    cells = inputs.make_cells(n, 23, "mixed")
+    atol, rtol = np.ones(59), np.full(59, 1e-3)
+    ys = []
+    for sched in (radm2b200.SCHED_STATIC, radm2b200.SCHED_PERSISTENT):
+        with radm2b200.Solver(schedule=sched) as s:
+            s.set_cells(cells)
+            s.update_rconst()
+            rc = s.get_rconst()
+            ipar, rpar = radm2b200.default_params(hstart=6.0)
+            assert s.rosenbrock(0.0, 600.0, atol, rtol, rpar, ipar) == 1
+            ys.append(s.get_state())
+    assert rel_err(ys[1], ys[0]).max() <= 1e-13
+    ipar, rpar = radm2b200.default_params(hstart=6.0)
+    ok, p = oracle.params(0.0, 600.0, atol, rtol, rpar, ipar)
+    y_o, _ = oracle.integrate(cells["VAR"], cells["FIX"], rc, p)
+    assert rel_err(ys[0], y_o).max() <= PARITY
