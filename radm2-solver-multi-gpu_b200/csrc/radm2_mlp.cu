@@ -411,19 +411,30 @@ __global__ void k_pack_weights(const float *__restrict__ p, __nv_bfloat16 *__res
 }
 
 // Features of each cell's current state (SoA cell arrays of a context).
-__global__ void k_features(int n, int ld, const double *__restrict__ var, const double *__restrict__ fix,
-                           const double *__restrict__ temp, const double *__restrict__ jv, float dt,
-                           float *__restrict__ f)
+// Features of a block of cells are formed in shared memory and written out as one
+// contiguous run of the row-major feature matrix (coalesced stores).
+constexpr int FEAT_BLOCK = 128, FEAT_PAD = NFEAT + 1;
+__global__ void __launch_bounds__(FEAT_BLOCK) k_features(int n, int ld, const double *__restrict__ var,
+                                                         const double *__restrict__ fix,
+                                                         const double *__restrict__ temp,
+                                                         const double *__restrict__ jv, float dt,
+                                                         float *__restrict__ f)
 {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= n) return;
-    float *o = f + (size_t)c * NFEAT;
-    for (int i = 0; i < NVAR; i++) o[i] = (float)log10(fmax(var[(size_t)i * ld + c], 1.0e-3));
-    o[59] = (float)temp[c];
-    o[60] = (float)log10(fmax(fix[(size_t)ld + c], 1.0));
-    o[61] = (float)log10(fmax(fix[c], 1.0));
-    for (int k = 0; k < RADM2_NJV_USED; k++) o[62 + k] = (float)log10(jv[(size_t)k * ld + c] + 1.0e-12);
-    o[83] = dt;
+    __shared__ float sf[FEAT_BLOCK * FEAT_PAD];
+    const int c0 = blockIdx.x * FEAT_BLOCK, c = c0 + threadIdx.x;
+    float *o = sf + threadIdx.x * FEAT_PAD;
+    if (c < n) {
+        for (int i = 0; i < NVAR; i++) o[i] = (float)log10(fmax(var[(size_t)i * ld + c], 1.0e-3));
+        o[59] = (float)temp[c];
+        o[60] = (float)log10(fmax(fix[(size_t)ld + c], 1.0));
+        o[61] = (float)log10(fmax(fix[c], 1.0));
+        for (int k = 0; k < RADM2_NJV_USED; k++) o[62 + k] = (float)log10(jv[(size_t)k * ld + c] + 1.0e-12);
+        o[83] = dt;
+    }
+    __syncthreads();
+    const int rows = min(FEAT_BLOCK, n - c0);
+    float *dst = f + (size_t)c0 * NFEAT;
+    for (int i = threadIdx.x; i < rows * NFEAT; i += FEAT_BLOCK) dst[i] = sf[(i / NFEAT) * FEAT_PAD + i % NFEAT];
 }
 
 // Predictions -> per-cell starting step (h0 = 10^(y0 * s0 + m0)) and a descending cost key.
@@ -618,8 +629,9 @@ cudaError_t radm2::mlp_enqueue_seed(radm2_ctx *c, radm2_mlp *m, double dt, int o
     const int n = count < 0 ? c->ncell : count;
     if (count >= 0) order = 0;
     (void)cudaGetLastError();
-    k_features<<<(n + 127) / 128, 128, 0, c->st>>>(n, c->ld, c->var + lo, c->fix + lo, c->temp + lo, c->jv + lo,
-                                                   (float)dt, c->seed_x);
+    k_features<<<(n + FEAT_BLOCK - 1) / FEAT_BLOCK, FEAT_BLOCK, 0, c->st>>>(n, c->ld, c->var + lo, c->fix + lo,
+                                                                         c->temp + lo, c->jv + lo, (float)dt,
+                                                                         c->seed_x);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = forward(m, n, c->seed_x, c->seed_y, false, c->st);
     if (e == cudaSuccess) {
@@ -833,7 +845,8 @@ int radm2_get_features(radm2_ctx *c, double dt, float *host_out)
     cudaSetDevice(c->o.device);
     float *d = nullptr;
     if (cudaMalloc(&d, sizeof(float) * (size_t)c->ncell * NFEAT) != cudaSuccess) return RADM2_E_NOMEM;
-    k_features<<<(c->ncell + 127) / 128, 128, 0, c->st>>>(c->ncell, c->ld, c->var, c->fix, c->temp, c->jv, (float)dt, d);
+    k_features<<<(c->ncell + FEAT_BLOCK - 1) / FEAT_BLOCK, FEAT_BLOCK, 0, c->st>>>(c->ncell, c->ld, c->var, c->fix,
+                                                                              c->temp, c->jv, (float)dt, d);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(host_out, d, sizeof(float) * (size_t)c->ncell * NFEAT,
                                               cudaMemcpyDeviceToHost, c->st);

@@ -32,6 +32,18 @@ def test_features_are_finite_and_shaped(feats):
     assert (feats[:, 83] == 600.0).all()
 
 
+def test_features_match_their_definition(feats):
+    c = inputs.make_cells(2048, 11, "mixed")
+    exp = np.empty((2048, 84))
+    exp[:, :59] = np.log10(np.maximum(c["VAR"], 1e-3))
+    exp[:, 59] = c["TEMP"]
+    exp[:, 60] = np.log10(np.maximum(c["FIX"][:, 1], 1.0))
+    exp[:, 61] = np.log10(np.maximum(c["FIX"][:, 0], 1.0))
+    exp[:, 62:83] = np.log10(c["JV"][:, :21] + 1e-12)
+    exp[:, 83] = 600.0
+    assert np.abs(feats - exp.astype(np.float32)).max() <= 2e-6 * np.abs(exp).max()
+
+
 def test_forward_matches_reference(feats):
     net, xm, xs = _net(feats)
     p = net.params()
