@@ -272,6 +272,17 @@ int radm2_mlp_train_step(radm2_mlp *mlp, int n, const float *x, const float *tar
 int radm2_mlp_synchronize(radm2_mlp *mlp);
 /* Safety factor on seeded starting steps: h0 = scale * predicted step (default 1). */
 int radm2_mlp_set_h0_scale(radm2_mlp *mlp, float scale);
+/* Inference forward (radm2_mlp_forward and the seeding of attached contexts) on the
+ * tcgen05 tensor cores with the accumulator in tensor memory (tcgen05 != 0, the default)
+ * or on mma.sync tiles (0).  Training always uses the mma.sync kernels, which keep the
+ * pre-activations for the backward pass.  No counterpart in the reference (its solver
+ * has no learned seeding). */
+int radm2_mlp_set_tensor_path(radm2_mlp *mlp, int tcgen05);
+/* RADM2_OK, or RADM2_E_CUDA once a tcgen05 forward gave up waiting on its tensor-core
+ * work (its predictions are then not to be used; the flag stays set).  Read it after the
+ * work has completed: radm2_mlp_forward checks it itself; for attached contexts call it
+ * after the integration returned. */
+int radm2_mlp_status(radm2_mlp *mlp);
 /* Features of the context's current cell states, host out[ncell][84]. */
 int radm2_get_features(radm2_ctx *ctx, double dt, float *out);
 /* Seed the context from the network: per-cell starting steps (set_h0) and, for the

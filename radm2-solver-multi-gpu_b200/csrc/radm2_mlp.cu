@@ -1,10 +1,11 @@
 // Step-seeding network: features of each cell's state -> (log h0, log accepted steps).
 //
 // MLP 96 (84 features, zero padded) -> 128 -> 128 -> 128 -> 8 (2 outputs, zero padded),
-// GELU hidden activations, BF16 weights and activations on the tensor cores
-// (mma.sync m16n8k16, FP32 accumulation), FP32 master weights and Adam moments.
-// Forward and backward are fused over all four layers: a CTA takes 64 samples, each of
-// its 4 warps 16 rows; weights live in shared memory (transposed, k contiguous).
+// GELU hidden activations, BF16 weights and activations on the tensor cores with FP32
+// accumulation, FP32 master weights and Adam moments.  Inference (k_forward_tc) issues
+// tcgen05.mma with the accumulators in tensor memory; training (k_forward keeping the
+// pre-activations, k_backward) uses mma.sync m16n8k16 tiles.  Forward and backward are
+// fused over all four layers; weights live in shared memory (transposed, k contiguous).
 #include <cuda_bf16.h>
 
 #include <cstring>
@@ -257,6 +258,277 @@ __device__ __forceinline__ void warp_gemm_wt(float (*acc)[4], const __nv_bfloat1
     }
 }
 
+// ---------------------------------------------------------------- tcgen05 forward
+// The inference forward on the 5th-generation tensor cores.  A CTA holds the transposed
+// weights once in shared memory and runs TC_G independent tile pipelines (4 warps each,
+// 128 rows per tile): per layer, one thread issues K/16 `tcgen05.mma.kind::f16`
+// (BF16 x BF16 -> FP32) with A = the tile's activations and B = the weights, both in the
+// canonical K-major no-swizzle layout, and D = a 128 x N FP32 accumulator in the pipeline's
+// 128 tensor-memory columns (lane = row).  `tcgen05.commit` arms the pipeline's mbarrier;
+// the epilogue reads D back with `tcgen05.ld` (warp w: lanes 32(w%4)..+31), adds the bias,
+// applies GELU and writes the next layer's BF16 activations in place (the MMA that read
+// them has completed).  While one pipeline waits on its MMAs the others run their
+// epilogues.  Every wait is bounded and reports through *err.
+//
+// Canonical K-major layout (no swizzle): element (r, k) of an [R][K] BF16 operand at byte
+// ((r / 8) * (K / 8) + k / 8) * 128 + (r % 8) * 16 + (k % 8) * 2: 8 x 16-byte core matrices,
+// K-adjacent ones 128 B apart (leading byte offset), 8-row groups K * 16 B apart (stride
+// byte offset).
+constexpr int TC_M = 128;                      // tile rows = TMEM lanes
+constexpr int TC_G = 4;                        // tile pipelines per CTA (4 warps each)
+constexpr int TC_THREADS = TC_G * TC_M;
+constexpr int TC_N4 = 16;                      // output layer N (2 outputs, padded)
+constexpr int TB_W1 = 0;                       // W1^T [128][96]
+constexpr int TB_W2 = TB_W1 + W * NIN * 2;     // W2^T [128][128]
+constexpr int TB_W3 = TB_W2 + W * W * 2;       // W3^T [128][128]
+constexpr int TB_W4 = TB_W3 + W * W * 2;       // W4^T [16][128]
+constexpr int TB_ACT = TB_W4 + TC_N4 * W * 2;  // per pipeline: activations [128][128] (layer 1 reads k < 96)
+constexpr int TB_BIAS = TB_ACT + TC_G * TC_M * W * 2;  // floats: 3 x 128 + 8
+constexpr int TB_NORM = TB_BIAS + (3 * W + NOUT) * 4;  // floats: mean[96], std[96]
+constexpr int TB_MBAR = TB_NORM + 2 * NIN * 4;         // per pipeline, 8 bytes
+constexpr int TB_TMEM = TB_MBAR + 8 * TC_G;
+constexpr int TB_FLAG = TB_TMEM + 4;                   // per pipeline: a wait gave up
+constexpr int TC_SMEM = TB_FLAG + 4 * TC_G;
+constexpr int TC_TMEM_COLS = 128 * TC_G;
+constexpr long TC_WAIT_LIMIT = 1L << 22;  // try_wait rounds before a wait gives up
+static_assert(TB_ACT % 16 == 0 && TB_W2 % 16 == 0 && TB_W4 % 16 == 0 && TB_MBAR % 8 == 0, "operand alignment");
+static_assert(TC_SMEM <= 227 * 1024, "tcgen05 forward shared memory");
+static_assert(TC_TMEM_COLS <= 512, "tensor memory columns");
+static_assert(NFEAT % 4 == 0 && NIN % 8 == 0, "feature rows in 16-byte groups");
+
+__host__ __device__ constexpr int canon_off(int r, int k, int K)
+{
+    return ((r >> 3) * (K >> 3) + (k >> 3)) * 128 + (r & 7) * 16 + (k & 7) * 2;
+}
+
+// Shared-memory matrix descriptor: start, leading (K) and stride (8-row) byte offsets in
+// 16-byte units, descriptor version 1, no swizzle.
+__host__ __device__ constexpr uint64_t umma_desc(uint32_t saddr, int K)
+{
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((128 >> 4) & 0x3FFF) << 16) |
+           ((uint64_t)(((K / 8) * 128 >> 4) & 0x3FFF) << 32) | ((uint64_t)1 << 46);
+}
+
+// Instruction descriptor: FP32 accumulator, BF16 A and B, both K-major, M x N.
+__host__ __device__ constexpr uint32_t umma_idesc(int M, int N)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+// Last byte a K=16 MMA step reads from an operand of `rows` rows laid out with extent K:
+// 8-row groups at stride K*16 B, two K-adjacent core matrices 128 B apart, 8 rows of 16 B.
+__host__ __device__ constexpr int umma_last_byte(int step, int rows, int K)
+{
+    return step * 256 + (rows / 8 - 1) * (K / 8) * 128 + 128 + 7 * 16 + 15;
+}
+static_assert(umma_last_byte(W / 16 - 1, TC_M, W) < TC_M * W * 2, "A operand inside its buffer");
+static_assert(umma_last_byte(NIN / 16 - 1, W, NIN) < W * NIN * 2, "W1 operand inside its buffer");
+static_assert(umma_last_byte(W / 16 - 1, W, W) < W * W * 2, "W2/W3 operand inside its buffer");
+static_assert(umma_last_byte(W / 16 - 1, TC_N4, W) < TC_N4 * W * 2, "W4 operand inside its buffer");
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t phase)
+{
+    for (long it = 0; it < TC_WAIT_LIMIT; it++) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, P1;\n\t}\n"
+            : "=r"(ok)
+            : "r"(addr), "r"(phase)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v)
+{
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void proxy_fence() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+// barrier of one tile pipeline's 4 warps (named barrier 1 + g)
+__device__ __forceinline__ void group_sync(int g) { asm volatile("bar.sync %0, %1;\n" ::"r"(1 + g), "r"(TC_M) : "memory"); }
+
+// Copy a transposed weight matrix WT[rows][k < kvalid] (row stride ks, bf16) into the
+// canonical layout [rows_pad][K]; rows and columns beyond the source are zero.
+__device__ void stage_canon(unsigned char *dst, const __nv_bfloat16 *src, int rows, int rows_pad, int kvalid, int ks,
+                            int K)
+{
+    for (int i = threadIdx.x; i < rows_pad * (K / 8); i += blockDim.x) {
+        const int r = i / (K / 8), k0 = (i % (K / 8)) * 8;
+        uint4 v = make_uint4(0, 0, 0, 0);
+        if (r < rows && k0 < kvalid) v = *reinterpret_cast<const uint4 *>(src + (size_t)r * ks + k0);
+        *reinterpret_cast<uint4 *>(dst + canon_off(r, k0, K)) = v;
+    }
+}
+
+__global__ void __launch_bounds__(TC_THREADS) k_forward_tc(Net net, int n, const float *__restrict__ x,
+                                                          float *__restrict__ y, int *__restrict__ err)
+{
+    extern __shared__ __align__(1024) unsigned char sm[];
+    float *sb = reinterpret_cast<float *>(sm + TB_BIAS);
+    float *snorm = reinterpret_cast<float *>(sm + TB_NORM);
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(sm + TB_TMEM);
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int g = warp >> 2, gt = tid & (TC_M - 1);  // pipeline, thread within it (= tile row)
+    volatile int *gflag = reinterpret_cast<volatile int *>(sm + TB_FLAG) + g;
+    const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(sm);
+    const uint32_t mbar = sbase + TB_MBAR + 8 * g;
+    unsigned char *act = sm + TB_ACT + g * (TC_M * W * 2);
+    const uint32_t act_s = sbase + TB_ACT + g * (TC_M * W * 2);
+
+    // weights (canonical, once per CTA), biases, normalisation
+    stage_canon(sm + TB_W1, net.wt + S_WT1, W, W, NIN, KP_IN, NIN);
+    stage_canon(sm + TB_W2, net.wt + S_WT2, W, W, W, KP, W);
+    stage_canon(sm + TB_W3, net.wt + S_WT3, W, W, W, KP, W);
+    stage_canon(sm + TB_W4, net.wt + S_WT4, NOUT, TC_N4, W, KP, W);
+    for (int i = tid; i < W; i += blockDim.x) {
+        sb[i] = net.params[OFF_B1 + i];
+        sb[W + i] = net.params[OFF_B2 + i];
+        sb[2 * W + i] = net.params[OFF_B3 + i];
+    }
+    for (int i = tid; i < NOUT; i += blockDim.x) sb[3 * W + i] = net.params[OFF_B4 + i];
+    for (int i = tid; i < NIN; i += blockDim.x) {
+        snorm[i] = net.xmean[i];
+        snorm[NIN + i] = net.xstd[i];
+    }
+    if (gt == 0) {
+        *gflag = 0;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(mbar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    // one warp owns the tensor-memory allocation; the shared-memory footprint keeps one CTA
+    // per SM and no other kernel of the library uses tensor memory, so the 512 columns are free
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(sbase + TB_TMEM),
+                     "r"(TC_TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+    }
+    proxy_fence();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot + (uint32_t)(128 * g);            // this pipeline's columns
+    const uint32_t trow = tmem + ((uint32_t)((warp & 3) * 32) << 16);  // this warp's lanes
+    uint32_t phase = 0;
+    const uint32_t idesc_h = umma_idesc(TC_M, W), idesc_o = umma_idesc(TC_M, TC_N4);
+    const int ntiles = (n + TC_M - 1) / TC_M;
+    const bool xvec = (reinterpret_cast<uintptr_t>(x) & 15) == 0;
+
+#pragma unroll 1
+    for (int tile = blockIdx.x * TC_G + g; tile < ntiles && !*gflag; tile += gridDim.x * TC_G) {
+        const int row0 = tile * TC_M;
+        // normalised inputs -> bf16 activations (k < 96; features >= 84 are zero)
+        for (int i = gt; i < TC_M * (NIN / 8); i += TC_M) {
+            const int r = i / (NIN / 8), k0 = (i % (NIN / 8)) * 8, gr = row0 + r;
+            float v[8];
+#pragma unroll
+            for (int q = 0; q < 2; q++) {  // rows are NFEAT * 4 = 336 bytes: 16-byte groups stay aligned
+                const int k = k0 + 4 * q;
+                float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (gr < n && k < NFEAT) {
+                    if (xvec) {
+                        f = __ldg(reinterpret_cast<const float4 *>(x + (size_t)gr * NFEAT + k));
+                    } else {
+                        const float *xs = x + (size_t)gr * NFEAT + k;
+                        f = make_float4(xs[0], xs[1], xs[2], xs[3]);
+                    }
+                }
+                v[4 * q] = f.x, v[4 * q + 1] = f.y, v[4 * q + 2] = f.z, v[4 * q + 3] = f.w;
+            }
+            uint32_t pk[4];
+#pragma unroll
+            for (int h = 0; h < 4; h++) {
+                const int k = k0 + 2 * h;
+                pk[h] = k < NFEAT ? pack_bf16((v[2 * h] - snorm[k]) / snorm[NIN + k],
+                                              (v[2 * h + 1] - snorm[k + 1]) / snorm[NIN + k + 1])
+                                  : 0u;
+            }
+            *reinterpret_cast<uint4 *>(act + canon_off(r, k0, W)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+        }
+        proxy_fence();
+        group_sync(g);
+#pragma unroll 1
+        for (int l = 0; l < 4; l++) {
+            const int K = l == 0 ? NIN : W;
+            const uint32_t b_off = l == 0 ? TB_W1 : l == 1 ? TB_W2 : l == 2 ? TB_W3 : TB_W4;
+            if (gt == 0) {
+                tc_fence_after();
+#pragma unroll 1
+                for (int s = 0; s < K / 16; s++)
+                    umma_bf16(tmem, umma_desc(act_s + s * 256, W), umma_desc(sbase + b_off + s * 256, K),
+                              l < 3 ? idesc_h : idesc_o, s > 0 ? 1u : 0u);
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                                 mbar)
+                             : "memory");
+            }
+            if (!mbar_wait(mbar, phase)) *gflag = 1;
+            group_sync(g);  // one decision for the pipeline
+            if (*gflag) break;
+            phase ^= 1u;
+            tc_fence_after();
+            if (l < 3) {  // bias + GELU -> bf16 activations of the next layer, in place
+#pragma unroll 1
+                for (int c0 = 0; c0 < W; c0 += 16) {
+                    float v[16];
+                    tmem_ld16(trow + c0, v);
+                    uint32_t pk[8];
+#pragma unroll
+                    for (int h = 0; h < 8; h++)
+                        pk[h] = pack_bf16(gelu(v[2 * h] + sb[l * W + c0 + 2 * h]),
+                                          gelu(v[2 * h + 1] + sb[l * W + c0 + 2 * h + 1]));
+                    *reinterpret_cast<uint4 *>(act + canon_off(gt, c0, W)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                    *reinterpret_cast<uint4 *>(act + canon_off(gt, c0 + 8, W)) =
+                        make_uint4(pk[4], pk[5], pk[6], pk[7]);
+                }
+            } else {  // outputs
+                float v[16];
+                tmem_ld16(trow, v);
+                const int gr = row0 + gt;
+                if (gr < n) {
+                    y[(size_t)gr * NY] = v[0] + sb[3 * W];
+                    y[(size_t)gr * NY + 1] = v[1] + sb[3 * W + 1];
+                }
+            }
+            tc_fence_before();
+            proxy_fence();
+            group_sync(g);
+        }
+    }
+    if (*gflag) {
+        if (gt == 0) atomicExch(err, 1);
+        // a wait that gave up may leave tensor-core work in flight: give it a bounded chance
+        // to finish before the accumulator memory is released
+        mbar_wait(mbar, phase);
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(*tmem_slot), "r"(TC_TMEM_COLS)
+                     : "memory");
+}
+
 // Backward for MSE loss mean over (n x NY): fills grad[NPARAM] (atomic sums over CTAs) and
 // adds the CTA's loss partial to *loss.
 __global__ void __launch_bounds__(128) k_backward(Net net, int n, const float *__restrict__ x,
@@ -502,6 +774,8 @@ struct radm2_mlp {
     float h0_scale = 1.0f;  // seeded h0 = h0_scale * predicted step
     unsigned int gen = 0;   // bumped when a value that seeding passes by value changes
     int attached = 0;       // contexts that seed every integration from this network
+    bool use_tc = true;     // inference forward on tcgen05 (else mma.sync)
+    int *tc_err = nullptr;  // device flag: a tcgen05 forward wait gave up
 };
 
 namespace {
@@ -549,6 +823,7 @@ cudaError_t set_kernel_attributes()
     if (done) return cudaSuccess;
     cudaError_t e = cudaFuncSetAttribute(k_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, FWD_SMEM_BYTES);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_forward_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
     done = e == cudaSuccess;
     return e;
 }
@@ -557,6 +832,13 @@ cudaError_t forward(radm2_mlp *m, int n, const float *dx, float *dy, bool keep, 
 {
     cudaError_t e0 = set_kernel_attributes();
     if (e0 != cudaSuccess) return e0;
+    (void)cudaGetLastError();
+    if (!keep && m->use_tc) {  // inference: tcgen05 pipelines of 128-row tiles, one CTA per SM
+        const int groups = (n + TC_M * TC_G - 1) / (TC_M * TC_G);
+        k_forward_tc<<<groups < m->nsm ? groups : m->nsm, TC_THREADS, TC_SMEM, st>>>(net_of(m), n, dx, dy,
+                                                                                   m->tc_err);
+        return cudaGetLastError();
+    }
     const size_t zs = (size_t)m->zcap * W;
     const int ntiles = (n + FWD_ROWS - 1) / FWD_ROWS;
     const int grid = ntiles < m->nsm ? ntiles : m->nsm;  // one CTA per SM walks the row tiles
@@ -680,7 +962,8 @@ int radm2_mlp_create(radm2_mlp **out, int device, unsigned int seed)
               cudaMalloc(&m->wt, sizeof(__nv_bfloat16) * S_WEND) == cudaSuccess &&
               cudaMalloc(&m->xmean, sizeof(float) * NIN) == cudaSuccess &&
               cudaMalloc(&m->xstd, sizeof(float) * NIN) == cudaSuccess &&
-              cudaMalloc(&m->loss, sizeof(float)) == cudaSuccess;
+              cudaMalloc(&m->loss, sizeof(float)) == cudaSuccess &&
+              cudaMalloc(&m->tc_err, sizeof(int)) == cudaSuccess;
     if (!ok) {
         radm2_mlp_destroy(m);
         return RADM2_E_NOMEM;
@@ -706,6 +989,7 @@ int radm2_mlp_create(radm2_mlp **out, int device, unsigned int seed)
          cudaMemset(m->g, 0, sizeof(float) * NPARAM) == cudaSuccess &&
          cudaMemset(m->m, 0, sizeof(float) * NPARAM) == cudaSuccess &&
          cudaMemset(m->v, 0, sizeof(float) * NPARAM) == cudaSuccess &&
+         cudaMemset(m->tc_err, 0, sizeof(int)) == cudaSuccess &&
          cudaMemcpy(m->xmean, zeros.data(), sizeof(float) * NIN, cudaMemcpyHostToDevice) == cudaSuccess &&
          cudaMemcpy(m->xstd, ones.data(), sizeof(float) * NIN, cudaMemcpyHostToDevice) == cudaSuccess &&
          pack(m) == cudaSuccess && cudaStreamSynchronize(m->st) == cudaSuccess;
@@ -723,7 +1007,8 @@ int radm2_mlp_destroy(radm2_mlp *m)
     if (m->attached > 0) return RADM2_E_STATE;  // still attached to a context
     cudaSetDevice(m->device);
     if (m->st) cudaStreamSynchronize(m->st);
-    void *ptrs[] = {m->p, m->g, m->m, m->v, m->wt, m->xmean, m->xstd, m->loss, m->z, m->y, m->xbuf, m->tbuf};
+    void *ptrs[] = {m->p,    m->g, m->m, m->v,    m->wt,   m->xmean, m->xstd,
+                    m->loss, m->z, m->y, m->xbuf, m->tbuf, m->tc_err};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     if (m->st) cudaStreamDestroy(m->st);
@@ -782,7 +1067,7 @@ int radm2_mlp_forward(radm2_mlp *m, int n, const float *x, float *y)
         cudaMemcpyAsync(y, m->y, sizeof(float) * (size_t)n * NY, cudaMemcpyDeviceToHost, m->st) != cudaSuccess ||
         cudaStreamSynchronize(m->st) != cudaSuccess)
         return RADM2_E_CUDA;
-    return RADM2_OK;
+    return radm2_mlp_status(m);
 }
 
 int radm2_mlp_gradients(radm2_mlp *m, int n, const float *x, const float *target, float *grad, float *loss)
@@ -830,6 +1115,23 @@ int radm2_mlp_set_h0_scale(radm2_mlp *m, float scale)
     m->h0_scale = scale;
     m->gen++;
     return RADM2_OK;
+}
+
+int radm2_mlp_set_tensor_path(radm2_mlp *m, int tcgen05)
+{
+    if (!m) return RADM2_E_ARG;
+    m->use_tc = tcgen05 != 0;
+    m->gen++;  // graphs that captured the other forward are rebuilt
+    return RADM2_OK;
+}
+
+int radm2_mlp_status(radm2_mlp *m)
+{
+    if (!m) return RADM2_E_ARG;
+    cudaSetDevice(m->device);
+    int flag = 0;
+    if (cudaMemcpy(&flag, m->tc_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return RADM2_E_CUDA;
+    return flag ? RADM2_E_CUDA : RADM2_OK;
 }
 
 int radm2_mlp_synchronize(radm2_mlp *m)

@@ -94,6 +94,8 @@ SIGNATURES = {
                                             ctypes.c_float, _F]),
     "radm2_mlp_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
     "radm2_mlp_set_h0_scale": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_float]),
+    "radm2_mlp_set_tensor_path": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "radm2_mlp_status": (ctypes.c_int, [ctypes.c_void_p]),
     "radm2_get_features": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, _F]),
     "radm2_seed_cells": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_int,
                                         ctypes.c_int]),
@@ -484,3 +486,12 @@ class Mlp:
 
     def set_h0_scale(self, scale):
         self._check(self.lib.radm2_mlp_set_h0_scale(self.h, scale))
+
+    def set_tensor_path(self, tcgen05=True):
+        """Inference forward on tcgen05 with tensor-memory accumulators (default) or on
+        mma.sync tiles; training always uses the mma.sync kernels."""
+        self._check(self.lib.radm2_mlp_set_tensor_path(self.h, 1 if tcgen05 else 0))
+
+    def status(self):
+        """Raise if a tcgen05 forward gave up waiting on its tensor-core work."""
+        self._check(self.lib.radm2_mlp_status(self.h))

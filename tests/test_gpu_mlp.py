@@ -171,3 +171,23 @@ def test_nonfinite_predictions_fall_back_to_default_step():
             s.attach_mlp(None)
     assert outs[0][1:] == outs[1][1:]
     assert np.array_equal(outs[0][0], outs[1][0])
+
+
+@pytest.mark.parametrize("n", [1000, 128, 37, 160037])
+def test_tcgen05_forward_matches_mma_sync_forward(feats, n):
+    """The inference forward on tcgen05 (accumulator in tensor memory) and on mma.sync tiles
+    compute the same network: equal up to the FP32 accumulation order.  160,037 rows give
+    every tile pipeline of a full grid several tiles and a ragged last one."""
+    x = np.ascontiguousarray(np.tile(feats, ((n + len(feats) - 1) // len(feats), 1))[:n])
+    net, xm, xs = _net(feats)
+    net.set_tensor_path(True)
+    y_tc = net.forward(x)
+    net.status()
+    net.set_tensor_path(False)
+    y_ms = net.forward(x)
+    assert np.isfinite(y_tc).all()
+    assert np.abs(y_tc - y_ms).max() <= 1e-3 * max(1.0, np.abs(y_ms).max())
+    p = net.params()
+    m = min(n, 1000)
+    y_ref, _, _ = mlp_ref.forward_backward(p, xm, xs, x[:m], bf=True)
+    assert np.abs(y_tc[:m] - y_ref).max() <= 1e-2 * max(1.0, np.abs(y_ref).max())
