@@ -69,6 +69,8 @@ def parse():
     ap.add_argument("--method", default="learned", choices=["learned", "plain"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32lu"])
     ap.add_argument("--schedule", default="persistent", choices=["static", "persistent"])
+    ap.add_argument("--refine", type=int, default=1, choices=[0, 1, 2],
+                    help="fp32lu: FP64 refinement sweeps per stage solve")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shape")
     ap.add_argument("--block-threads", type=int, default=0)
     ap.add_argument("--blocks-per-sm", type=int, default=0)
@@ -275,7 +277,7 @@ def main():
     cells = inputs.make_cells(ncell, seed, wl, night, first_cell=rank * ncell)
     prec = radm2b200.PREC_FP32LU if args.precision == "fp32lu" else radm2b200.PREC_FP64
     sched = radm2b200.SCHED_PERSISTENT if args.schedule == "persistent" else radm2b200.SCHED_STATIC
-    refine = 1
+    refine = args.refine
     atol, rtol = np.full(59, ATOL), np.full(59, RTOL)
     stream = torch.cuda.Stream()
     ld = (ncell + 31) // 32 * 32
@@ -474,7 +476,7 @@ def main():
             peaks = json.load(f)
     hbm = peaks.get("hbm_gbs")
     method = ("learned step seeding (network in the split graph) + persistent work stealing"
-              if learned else "plain") + (", FP32 Jacobian/LU + FP64 refinement" if prec else ", FP64")
+              if learned else "plain") + (", FP32 Jacobian/LU + %d FP64 refinement sweep(s)" % refine if prec else ", FP64")
     line = {
         "metric": "chem cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": main_arm["el_ms"] / args.steps,
