@@ -59,6 +59,10 @@ WORKLOADS = {
 ATOL, RTOL, RTOL_TIGHT = 1.0, 1.0e-3, 1.0e-8
 
 
+# HBM copy bandwidth of a B200 when no measured peak file is present (GB/s).
+HBM_FALLBACK_GBS = 6650.0
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -475,6 +479,9 @@ def main():
         with open(pfile) as f:
             peaks = json.load(f)
     hbm = peaks.get("hbm_gbs")
+    hbm_source = "measured (MEASURED_PEAKS.json)"
+    if not hbm:
+        hbm, hbm_source = HBM_FALLBACK_GBS, "fallback (earlier copy-bandwidth measurement on B200)"
     method = ("learned step seeding (network in the split graph) + persistent work stealing"
               if learned else "plain") + (", FP32 Jacobian/LU + %d FP64 refinement sweep(s)" % refine if prec else ", FP64")
     line = {
@@ -498,7 +505,8 @@ def main():
                      "kernel": "k_rosenbrock (solver)",
                      "kernel_ms_per_launch": kms / max(klaunch, 1), "flops_per_launch": per_launch_flops,
                      "traffic_gbs": traffic_gbs,
-                     "traffic_frac_of_hbm": (traffic_gbs / hbm) if (traffic_gbs and hbm) else None},
+                     "traffic_frac_of_hbm": (traffic_gbs / hbm) if (traffic_gbs and hbm) else None,
+                     "hbm_peak_gbs": hbm, "hbm_peak_source": hbm_source},
         "steps_per_cell": {"accepted": main_arm["acc"] / (ncell * world) / args.steps,
                            "rejected": main_arm["rej"] / (ncell * world) / args.steps},
         "clocks": main_arm["clocks"],
