@@ -326,3 +326,66 @@ def test_mixed_regime_parity():
           % (e.max(), int((e.max(1) > 1e-10).sum()), int((e.max(1) > 1e-12).sum())))
     assert np.array_equal(st["nacc"], st_o["nacc"]) and np.array_equal(st["nrej"], st_o["nrej"])
     assert e.max() <= 1e-9
+
+
+def _parity_case(sub, tstart, tend, atol, rtol, ipar, rpar):
+    """GPU (persistent schedule) and oracle on the same cells, rate constants and
+    parameters; returns both results and both sets of statistics."""
+    with radm2b200.Solver(schedule=radm2b200.SCHED_PERSISTENT) as s:
+        s.set_cells(sub)
+        s.update_rconst()
+        rc = s.get_rconst()
+        ip, rp = ipar.copy(), rpar.copy()
+        ierr = s.rosenbrock(tstart, tend, atol, rtol, rp, ip)
+        y, st = s.get_state(), s.cell_stats()
+    ok, p = oracle.params(tstart, tend, atol, rtol, rpar, ipar)
+    assert ok == 1
+    y_o, st_o = oracle.integrate(sub["VAR"], sub["FIX"], rc, p)
+    return ierr, y, st, ip, rp, y_o, st_o
+
+
+def test_species_tolerances_and_control_parameters(cells4k):
+    """Per-species AbsTol/RelTol (IPAR[1] = 0), every step-control parameter away from its
+    default (Hmin, Hmax, Hstart, FacMin, FacMax, FacRej, FacSafe) and a window that does
+    not start at 0: the same steps and states as the oracle (mgpu.cu:3734-3791)."""
+    sub = {k: v[:1024] for k, v in cells4k.items()}
+    rng = np.random.default_rng(11)
+    atol = 10.0 ** rng.uniform(-1.0, 1.0, 59)
+    rtol = 10.0 ** rng.uniform(-4.0, -2.0, 59)
+    ipar, rpar = radm2b200.default_params(hstart=2.0)
+    rpar[0], rpar[1], rpar[3], rpar[4], rpar[5], rpar[6] = 1e-3, 240.0, 0.3, 4.0, 0.2, 0.85
+    ierr, y, st, ip, rp, y_o, st_o = _parity_case(sub, 3600.0, 4200.0, atol, rtol, ipar, rpar)
+    assert ierr == 1 and (st_o["status"] == 1).all()
+    assert np.array_equal(st["nacc"], st_o["nacc"]) and np.array_equal(st["nrej"], st_o["nrej"])
+    assert rel_err(y, y_o).max() <= PARITY
+    assert ip[13] == st_o["nacc"].sum() and ip[14] == st_o["nrej"].sum()
+    assert rp[10] == 4200.0
+
+
+def test_scalar_tolerances_use_first_entry(cells4k):
+    """IPAR[1] != 0: AbsTol[0] and RelTol[0] apply to every species (the rest of the arrays
+    is ignored), as in the oracle."""
+    sub = {k: v[:512] for k, v in cells4k.items()}
+    atol = np.concatenate([[0.5], np.full(58, 1e6)])
+    rtol = np.concatenate([[3e-4], np.full(58, 0.5)])
+    ipar, rpar = radm2b200.default_params(hstart=6.0)
+    ipar[1] = 1
+    ierr, y, st, _, _, y_o, st_o = _parity_case(sub, 0.0, 600.0, atol, rtol, ipar, rpar)
+    assert ierr == 1
+    assert np.array_equal(st["nacc"], st_o["nacc"]) and np.array_equal(st["nrej"], st_o["nrej"])
+    assert rel_err(y, y_o).max() <= PARITY
+    # and it equals the run with uniform arrays of those values
+    ipar[1] = 0
+    _, y_u, st_u, _, _, _, _ = _parity_case(sub, 0.0, 600.0, np.full(59, 0.5), np.full(59, 3e-4), ipar, rpar)
+    assert np.array_equal(y, y_u) and np.array_equal(st["nacc"], st_u["nacc"])
+
+
+def test_backward_window_reports_minus7_like_the_oracle(cells4k):
+    """Tend < Tstart integrates backwards (direction -1, mgpu.cu:3475-3477 and the mirrored
+    time-loop test).  The stiff chemistry is unstable backwards: the oracle ends every cell
+    with status -7 (step size too small); the GPU must report the same per cell and IERR -7."""
+    sub = {k: v[:256] for k, v in cells4k.items()}
+    ipar, rpar = radm2b200.default_params(hstart=1.0)
+    ierr, y, st, ip, rp, y_o, st_o = _parity_case(sub, 600.0, 540.0, ATOL, RTOL, ipar, rpar)
+    assert (st_o["status"] == -7).all()
+    assert ierr == -7 and np.array_equal(st["status"], st_o["status"])
