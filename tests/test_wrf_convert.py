@@ -59,3 +59,34 @@ def test_reference_text_files_round_trip(tmp_path):
     g = wrf_io.load_text_fields(str(tmp_path), dims=(5, 3, 6))
     for k in ("ph", "chem", "rad", "phy", "moist"):
         assert np.array_equal(f[k], g[k]), k
+
+
+def test_binary_fields_round_trip_and_text_conversion(tmp_path):
+    """The binary form holds exactly the arrays of the text files (read, mapped, or
+    converted from a text directory) and rejects a truncated or foreign file."""
+    from radm2b200 import wrf_io
+    f = inputs.make_wrf_fields(10, ni=6, nk=3, nj=5)
+    keys = ("ph", "chem", "rad", "phy", "moist")
+    wrf_io.save_binary_fields(f, str(tmp_path / "bin"))
+    for mmap in (False, True):
+        g = wrf_io.load_binary_fields(str(tmp_path / "bin"), mmap=mmap)
+        for k in keys:
+            assert g[k].shape == f[k].shape and np.array_equal(np.asarray(g[k]), f[k]), k
+    wrf_io.save_text_fields(f, str(tmp_path / "txt"))
+    wrf_io.text_to_binary(str(tmp_path / "txt"), str(tmp_path / "conv"), dims=(5, 3, 6))
+    h = wrf_io.load_binary_fields(str(tmp_path / "conv"))
+    for k in keys:
+        assert np.array_equal(h[k], f[k]), k
+    # the converted fields feed the conversion exactly like the originals
+    grid = (5, 3, 6, 1, 0, 1, 3, 2, 3)
+    a, b = oracle.convert_wrf(f, grid), oracle.convert_wrf(h, grid)
+    for key in KEYS:
+        assert np.array_equal(a[key], b[key]), key
+    chem = tmp_path / "bin" / "wrfchem.bin"
+    data = chem.read_bytes()
+    chem.write_bytes(data[:-8])
+    with pytest.raises(ValueError):
+        wrf_io.load_binary_fields(str(tmp_path / "bin"))
+    chem.write_bytes(b"NOTAWRF!" + data[8:])
+    with pytest.raises(ValueError):
+        wrf_io.load_binary_fields(str(tmp_path / "bin"))
