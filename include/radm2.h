@@ -283,6 +283,11 @@ int radm2_mlp_set_tensor_path(radm2_mlp *mlp, int tcgen05);
  * work has completed: radm2_mlp_forward checks it itself; for attached contexts call it
  * after the integration returned. */
 int radm2_mlp_status(radm2_mlp *mlp);
+/* Self-test of the tcgen05 forward's bounded waits: one launch that issues no tensor-core
+ * work, so its mbarrier waits run out after a short limit.  RADM2_OK when the kernel
+ * returned and raised the status flag (cleared again before returning), RADM2_E_STATE if
+ * it did not raise it.  The network stays usable.  No counterpart in the reference. */
+int radm2_mlp_selftest_wait_limit(radm2_mlp *mlp);
 /* Features of the context's current cell states, host out[ncell][84]. */
 int radm2_get_features(radm2_ctx *ctx, double dt, float *out);
 /* Seed the context from the network: per-cell starting steps (set_h0) and, for the

@@ -290,7 +290,9 @@ constexpr int TB_TMEM = TB_MBAR + 8 * TC_G;
 constexpr int TB_FLAG = TB_TMEM + 4;                   // per pipeline: a wait gave up
 constexpr int TC_SMEM = TB_FLAG + 4 * TC_G;
 constexpr int TC_TMEM_COLS = 128 * TC_G;
-constexpr long TC_WAIT_LIMIT = 1L << 22;  // try_wait rounds before a wait gives up
+constexpr long TC_WAIT_LIMIT = 1L << 22;         // try_wait rounds before a wait gives up
+constexpr long long TC_WAIT_CYCLES = 4000000000LL;  // and SM cycles (~2 s): a try_wait round
+                                                    // may suspend for a hardware-defined time
 static_assert(TB_ACT % 16 == 0 && TB_W2 % 16 == 0 && TB_W4 % 16 == 0 && TB_MBAR % 8 == 0, "operand alignment");
 static_assert(TC_SMEM <= 227 * 1024, "tcgen05 forward shared memory");
 static_assert(TC_TMEM_COLS <= 512, "tensor memory columns");
@@ -334,9 +336,10 @@ __device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t
         "l"(da), "l"(db), "r"(idesc), "r"(acc));
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t phase)
+__device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t phase, long limit)
 {
-    for (long it = 0; it < TC_WAIT_LIMIT; it++) {
+    const long long t0 = clock64();
+    for (long it = 0; it < limit && clock64() - t0 < TC_WAIT_CYCLES; it++) {
         uint32_t ok;
         asm volatile(
             "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
@@ -381,8 +384,12 @@ __device__ void stage_canon(unsigned char *dst, const __nv_bfloat16 *src, int ro
     }
 }
 
+// wait_limit bounds every mbarrier wait (TC_WAIT_LIMIT in production).  idle != 0 is the
+// self-test of that bound: no tensor-core work is issued or committed, so the first wait of
+// every pipeline runs out, raises *err and the kernel returns with nothing in flight.
 __global__ void __launch_bounds__(TC_THREADS) k_forward_tc(Net net, int n, const float *__restrict__ x,
-                                                          float *__restrict__ y, int *__restrict__ err)
+                                                          float *__restrict__ y, int *__restrict__ err,
+                                                          long wait_limit, int idle)
 {
     extern __shared__ __align__(1024) unsigned char sm[];
     float *sb = reinterpret_cast<float *>(sm + TB_BIAS);
@@ -472,7 +479,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_forward_tc(Net net, int n, const
         for (int l = 0; l < 4; l++) {
             const int K = l == 0 ? NIN : W;
             const uint32_t b_off = l == 0 ? TB_W1 : l == 1 ? TB_W2 : l == 2 ? TB_W3 : TB_W4;
-            if (gt == 0) {
+            if (gt == 0 && !idle) {
                 tc_fence_after();
 #pragma unroll 1
                 for (int s = 0; s < K / 16; s++)
@@ -482,7 +489,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_forward_tc(Net net, int n, const
                                  mbar)
                              : "memory");
             }
-            if (!mbar_wait(mbar, phase)) *gflag = 1;
+            if (!mbar_wait(mbar, phase, wait_limit)) *gflag = 1;
             group_sync(g);  // one decision for the pipeline
             if (*gflag) break;
             phase ^= 1u;
@@ -519,7 +526,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_forward_tc(Net net, int n, const
         if (gt == 0) atomicExch(err, 1);
         // a wait that gave up may leave tensor-core work in flight: give it a bounded chance
         // to finish before the accumulator memory is released
-        mbar_wait(mbar, phase);
+        mbar_wait(mbar, phase, wait_limit);
     }
     tc_fence_before();
     __syncthreads();
@@ -836,7 +843,7 @@ cudaError_t forward(radm2_mlp *m, int n, const float *dx, float *dy, bool keep, 
     if (!keep && m->use_tc) {  // inference: tcgen05 pipelines of 128-row tiles, one CTA per SM
         const int groups = (n + TC_M * TC_G - 1) / (TC_M * TC_G);
         k_forward_tc<<<groups < m->nsm ? groups : m->nsm, TC_THREADS, TC_SMEM, st>>>(net_of(m), n, dx, dy,
-                                                                                   m->tc_err);
+                                                                                   m->tc_err, TC_WAIT_LIMIT, 0);
         return cudaGetLastError();
     }
     const size_t zs = (size_t)m->zcap * W;
@@ -1132,6 +1139,25 @@ int radm2_mlp_status(radm2_mlp *m)
     int flag = 0;
     if (cudaMemcpy(&flag, m->tc_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return RADM2_E_CUDA;
     return flag ? RADM2_E_CUDA : RADM2_OK;
+}
+
+int radm2_mlp_selftest_wait_limit(radm2_mlp *m)
+{
+    if (!m) return RADM2_E_ARG;
+    cudaSetDevice(m->device);
+    int rc = mlp_ensure(m, TC_M, false);
+    if (rc) return rc;
+    if (set_kernel_attributes() != cudaSuccess) return RADM2_E_CUDA;
+    int raised = 0;
+    const int zero = 0;
+    // one CTA, one tile, nothing committed: every wait gives up after 4096 polls
+    (void)cudaGetLastError();
+    k_forward_tc<<<1, TC_THREADS, TC_SMEM, m->st>>>(net_of(m), TC_M, m->xbuf, m->y, m->tc_err, 4096L, 1);
+    if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(m->st) != cudaSuccess ||
+        cudaMemcpy(&raised, m->tc_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(m->tc_err, &zero, sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+        return RADM2_E_CUDA;
+    return raised ? RADM2_OK : RADM2_E_STATE;
 }
 
 int radm2_mlp_synchronize(radm2_mlp *m)

@@ -96,6 +96,7 @@ SIGNATURES = {
     "radm2_mlp_set_h0_scale": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_float]),
     "radm2_mlp_set_tensor_path": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "radm2_mlp_status": (ctypes.c_int, [ctypes.c_void_p]),
+    "radm2_mlp_selftest_wait_limit": (ctypes.c_int, [ctypes.c_void_p]),
     "radm2_get_features": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, _F]),
     "radm2_seed_cells": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_int,
                                         ctypes.c_int]),
@@ -495,3 +496,8 @@ class Mlp:
     def status(self):
         """Raise if a tcgen05 forward gave up waiting on its tensor-core work."""
         self._check(self.lib.radm2_mlp_status(self.h))
+
+    def selftest_wait_limit(self):
+        """Run the tcgen05 forward with no tensor-core work issued: its bounded waits must
+        run out, raise the status flag (cleared afterwards) and return."""
+        self._check(self.lib.radm2_mlp_selftest_wait_limit(self.h))

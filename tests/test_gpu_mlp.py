@@ -191,3 +191,20 @@ def test_tcgen05_forward_matches_mma_sync_forward(feats, n):
     m = min(n, 1000)
     y_ref, _, _ = mlp_ref.forward_backward(p, xm, xs, x[:m], bf=True)
     assert np.abs(y_tc[:m] - y_ref).max() <= 1e-2 * max(1.0, np.abs(y_ref).max())
+
+
+def test_tcgen05_wait_limit_reports_and_recovers(feats):
+    """A tcgen05 forward whose tensor-core work never completes (none is issued) gives up
+    after its bounded waits, reports through the status flag and leaves the network usable:
+    the next forward is correct and its status is clean."""
+    import time
+    net, _, _ = _net(feats)
+    net.set_tensor_path(True)
+    y0 = net.forward(feats[:256])
+    t0 = time.perf_counter()
+    net.selftest_wait_limit()
+    assert time.perf_counter() - t0 < 30.0
+    net.status()  # the self-test cleared its flag
+    y1 = net.forward(feats[:256])
+    net.status()
+    assert np.array_equal(y0, y1)
