@@ -705,8 +705,25 @@ int radm2_rosenbrock_host(radm2_ctx *c, int ncell, double *VAR, const double *FI
     const bool order_was = c->use_order;
     c->use_order = false;  // a chunk's cells are integrated in index order
     const double dt = std::fabs(p.Tend - p.Tstart);
+    // Chunk sizes: with three or more chunks the first and the last are a fifth of a middle
+    // one.  Only the first chunk's upload and the last chunk's download are not hidden
+    // behind an integration, and a cell's copies take a fraction of its integration time,
+    // so small edge chunks still cover the middle chunks' copies.
+    std::vector<size_t> bound(nchunk + 1, 0);
+    {
+        const double edge = nchunk >= 3 ? 0.2 : 1.0, total = 2.0 * edge + (nchunk - 2 > 0 ? nchunk - 2 : 0);
+        double acc = 0.0;
+        for (int k = 0; k < nchunk; k++) {
+            acc += (k == 0 || k == nchunk - 1) ? edge : 1.0;
+            bound[k + 1] = (k == nchunk - 1) ? n : (size_t)((double)n * (acc / total));
+        }
+        bool ok = true;
+        for (int k = 0; k < nchunk; k++) ok = ok && bound[k + 1] > bound[k];
+        if (!ok)  // (not reached: a chunk holds at least 1024 cells) equal chunks
+            for (int k = 0; k <= nchunk; k++) bound[k] = n * (size_t)k / (size_t)nchunk;
+    }
     for (int k = 0; k < nchunk; k++) {
-        const int lo = (int)(n * k / nchunk), hi = (int)(n * (k + 1) / nchunk), m = hi - lo;
+        const int lo = (int)bound[k], hi = (int)bound[k + 1], m = hi - lo;
         const size_t l = (size_t)lo;
         // up: copies of this chunk's rows, then the transposes into the cell arrays
         CK(cudaMemcpyAsync(sv + l * NVAR, VAR + l * NVAR, sizeof(double) * m * NVAR, cudaMemcpyHostToDevice, c->st_up));
