@@ -233,7 +233,9 @@ int radm2_get_opts(const radm2_ctx *ctx, radm2_opts *out);  /* options in force 
  * schedules x block size x placement of the working set (global scratch / shared memory)
  * x register cap -- on a strided sample of the context's current cells (sample_cells;
  * 0 = 262,144) for one split of length dt with the given tolerances and parameters, and
- * keeps the fastest in the context's options (radm2_get_opts reads them).  The context's
+ * keeps the fastest in the context's options (radm2_get_opts reads them).  Candidates
+ * within 2x of the best first-pass time are timed a second time and keep the faster of
+ * their two times, so a one-off slow measurement does not decide the choice.  The context's
  * cells and state are not changed.  table (may be NULL) receives up to table_len
  * entries, n_entries the number of candidates. */
 typedef struct radm2_tune_entry {
