@@ -224,6 +224,8 @@ cudaError_t variant_info(radm2_ctx *c, int bs, SolverInfo *info)
     const bool fp32 = c->o.precision == RADM2_PREC_FP32LU;
     const bool pers = c->o.schedule == RADM2_SCHED_PERSISTENT;
     const int k = key_of(c, bs);
+    if (fp32 && c->o.refine_sweeps == 0)
+        return pers ? solver_info_fp32d_persistent(k, info) : solver_info_fp32d_static(k, info);
     if (fp32) return pers ? solver_info_fp32_persistent(k, info) : solver_info_fp32_static(k, info);
     return pers ? solver_info_fp64_persistent(k, info) : solver_info_fp64_static(k, info);
 }
@@ -303,6 +305,8 @@ cudaError_t launch_solver(radm2_ctx *c, const SolveArgs &a, int bs, int grid)
     const bool fp32 = c->o.precision == RADM2_PREC_FP32LU;
     const bool pers = c->o.schedule == RADM2_SCHED_PERSISTENT;
     const int k = key_of(c, bs);
+    if (fp32 && c->o.refine_sweeps == 0)  // the variants without the refinement code
+        return pers ? launch_solver_fp32d_persistent(a, k, grid, c->st) : launch_solver_fp32d_static(a, k, grid, c->st);
     if (fp32)
         return pers ? launch_solver_fp32_persistent(a, k, grid, c->st) : launch_solver_fp32_static(a, k, grid, c->st);
     return pers ? launch_solver_fp64_persistent(a, k, grid, c->st) : launch_solver_fp64_static(a, k, grid, c->st);
@@ -1183,7 +1187,8 @@ int radm2_selfcheck(void)
 {
     // Layout bounds of every solver variant (host arithmetic only, no device needed).
     const int bad = solver_layout_check_fp64_static() | solver_layout_check_fp64_persistent() |
-                    solver_layout_check_fp32_static() | solver_layout_check_fp32_persistent();
+                    solver_layout_check_fp32_static() | solver_layout_check_fp32_persistent() |
+                    solver_layout_check_fp32d_static() | solver_layout_check_fp32d_persistent();
     return bad ? RADM2_E_STATE : RADM2_OK;
 }
 

@@ -68,14 +68,21 @@ cudaError_t launch_solver_fp64_static(const SolveArgs &a, int key, int grid, cud
 cudaError_t launch_solver_fp64_persistent(const SolveArgs &a, int key, int grid, cudaStream_t st);
 cudaError_t launch_solver_fp32_static(const SolveArgs &a, int key, int grid, cudaStream_t st);
 cudaError_t launch_solver_fp32_persistent(const SolveArgs &a, int key, int grid, cudaStream_t st);
+// FP32 LU without the refinement code (refine_sweeps = 0); same variant keys as fp32.
+cudaError_t launch_solver_fp32d_static(const SolveArgs &a, int key, int grid, cudaStream_t st);
+cudaError_t launch_solver_fp32d_persistent(const SolveArgs &a, int key, int grid, cudaStream_t st);
 cudaError_t solver_info_fp64_static(int key, SolverInfo *out);
 cudaError_t solver_info_fp64_persistent(int key, SolverInfo *out);
 cudaError_t solver_info_fp32_static(int key, SolverInfo *out);
 cudaError_t solver_info_fp32_persistent(int key, SolverInfo *out);
+cudaError_t solver_info_fp32d_static(int key, SolverInfo *out);
+cudaError_t solver_info_fp32d_persistent(int key, SolverInfo *out);
 // Host-side bounds check of every built variant's working-set layout (0 = all in bounds).
 int solver_layout_check_fp64_static();
 int solver_layout_check_fp64_persistent();
 int solver_layout_check_fp32_static();
 int solver_layout_check_fp32_persistent();
+int solver_layout_check_fp32d_static();
+int solver_layout_check_fp32d_persistent();
 
 }  // namespace radm2

@@ -179,8 +179,11 @@ __device__ RADM2_PHASE int ph_decomp(LUT *sg)
 //            right-hand side F + C31/h K1 is parked in K3)
 //   stage 2: (F + C31/h K1) + C32/h K2
 // FP64 LU: one substitution.  FP32 LU: the substitution in float, then `refine`
-// sweeps of x += G32^-1 (b - G64 x), residual in FP64 (G64 x = ghinv x - J x).
-template <int BS, typename LUT>
+// sweeps of x += G32^-1 (b - G64 x), residual in FP64 (G64 x = ghinv x - J x).  IR = 0
+// compiles the FP32 form without the refinement code (refine must be 0): the residual's
+// Jacobian-vector product and second substitution would otherwise stay in the kernel's
+// instruction footprint although they never run.
+template <int BS, typename LUT, int IR>
 __device__ RADM2_PHASE void ph_stage(int stage, const double *y, const double *rc, double *vec, const LUT *sg,
                                       double fix0, double fix1, double hc21, double hc31, double hc32,
                                       double ghinv, int refine)
@@ -213,7 +216,7 @@ __device__ RADM2_PHASE void ph_stage(int stage, const double *y, const double *r
         float xf[NVAR];
 #pragma unroll
         for (int i = 0; i < NVAR; i++) {
-            VW(VEC_TMP + i) = x[i];
+            if (IR) VW(VEC_TMP + i) = x[i];  // b, for the residual
             xf[i] = (float)x[i];
         }
 #define X(i) xf[i]
@@ -223,7 +226,7 @@ __device__ RADM2_PHASE void ph_stage(int stage, const double *y, const double *r
         for (int i = 0; i < NVAR; i++) x[i] = (double)xf[i];
         double *kout = vec + (VEC_K1 + stage * NVAR) * BS;
 #pragma unroll 1
-        for (int sweep = 0; sweep < refine; sweep++) {
+        for (int sweep = 0; sweep < (IR ? refine : 0); sweep++) {
             // park x in the stage's output slot so the residual reads it from memory
 #pragma unroll
             for (int i = 0; i < NVAR; i++) kout[i * BS] = x[i];
@@ -271,7 +274,7 @@ __device__ unsigned long long phase_clocks[1 << 16][8];
 #define PCLK(ph) do { } while (0)
 #endif
 
-template <int BS, typename LUT, int SCHED, int PLACE, int MINB>
+template <int BS, typename LUT, int SCHED, int PLACE, int MINB, int IR = 1>
 __global__ void __launch_bounds__(BS, MINB) k_rosenbrock(const SolveArgs a)
 {
     using L = Layout<LUT, PLACE>;
@@ -414,7 +417,7 @@ __global__ void __launch_bounds__(BS, MINB) k_rosenbrock(const SolveArgs a)
 
 #pragma unroll 1
         for (int stage = 0; stage < 3; stage++) {
-            ph_stage<BS, LUT>(stage, rcy + RCY_Y * BS, rcy + RCY_RC * BS, vec, sg, fix0, fix1, hc21, hc31, hc32, ghinv,
+            ph_stage<BS, LUT, IR>(stage, rcy + RCY_Y * BS, rcy + RCY_RC * BS, vec, sg, fix0, fix1, hc21, hc31, hc32, ghinv,
                               a.refine);
             PCLK(3 + stage);
         }

@@ -8,10 +8,10 @@
 
 namespace radm2 {
 
-template <int BS, typename LUT, int SCHED, int PLACE, int MINB>
+template <int BS, typename LUT, int SCHED, int PLACE, int MINB, int IR>
 cudaError_t launch_one(const SolveArgs &a, int grid, cudaStream_t st)
 {
-    auto k = k_rosenbrock<BS, LUT, SCHED, PLACE, MINB>;
+    auto k = k_rosenbrock<BS, LUT, SCHED, PLACE, MINB, IR>;
     const size_t smem = (size_t)Layout<LUT, PLACE>::smem_words * sizeof(double) * BS;
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -22,10 +22,10 @@ cudaError_t launch_one(const SolveArgs &a, int grid, cudaStream_t st)
     return cudaGetLastError();
 }
 
-template <int BS, typename LUT, int SCHED, int PLACE, int MINB>
+template <int BS, typename LUT, int SCHED, int PLACE, int MINB, int IR>
 cudaError_t info_one(SolverInfo *out)
 {
-    auto k = k_rosenbrock<BS, LUT, SCHED, PLACE, MINB>;
+    auto k = k_rosenbrock<BS, LUT, SCHED, PLACE, MINB, IR>;
     const size_t smem = (size_t)Layout<LUT, PLACE>::smem_words * sizeof(double) * BS;
     cudaFuncAttributes at{};
     cudaError_t e = cudaFuncGetAttributes(&at, k);
@@ -54,13 +54,17 @@ int check_one()
 }  // namespace radm2
 
 // The built (block size, placement, min blocks) lists, RADM2_VARIANTS_FP64 / _FP32, are in
-// radm2_internal.h (the autotuner walks them too).
+// radm2_internal.h (the autotuner walks them too).  An instantiation file sets RADM2_T
+// (LU type), RADM2_S (schedule) and, for FP32 LU without the refinement code, RADM2_IR 0.
+#ifndef RADM2_IR
+#define RADM2_IR 1
+#endif
 
 #define RADM2_KEY(BS_, PL_, MB_) ((BS_) * 64 + (MB_) * 4 + (PL_))
 #define RADM2_CASE_LAUNCH(BS_, PL_, MB_) \
-    case RADM2_KEY(BS_, PL_, MB_): return launch_one<BS_, RADM2_T, RADM2_S, PL_, MB_>(a, grid, st);
+    case RADM2_KEY(BS_, PL_, MB_): return launch_one<BS_, RADM2_T, RADM2_S, PL_, MB_, RADM2_IR>(a, grid, st);
 #define RADM2_CASE_INFO(BS_, PL_, MB_) \
-    case RADM2_KEY(BS_, PL_, MB_): return info_one<BS_, RADM2_T, RADM2_S, PL_, MB_>(out);
+    case RADM2_KEY(BS_, PL_, MB_): return info_one<BS_, RADM2_T, RADM2_S, PL_, MB_, RADM2_IR>(out);
 #define RADM2_CHECK(BS_, PL_, MB_) bad |= check_one<BS_, RADM2_T, RADM2_S, PL_, MB_>();
 
 #define RADM2_DEFINE_SOLVER(NAME, LIST)                                                                  \

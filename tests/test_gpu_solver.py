@@ -195,6 +195,33 @@ def test_fp32_lu_accuracy(cells4k):
     assert e32.max() <= e64.max() * 1.01 + 1e-9
 
 
+@pytest.mark.parametrize("schedule", [radm2b200.SCHED_STATIC, radm2b200.SCHED_PERSISTENT])
+def test_fp32_lu_without_refinement(cells4k, schedule):
+    """FP32 Jacobian/LU with no refinement sweep (refine_sweeps = 0, the kernels built
+    without the refinement code).  Gate against the plain FP64 solver at the same rtol:
+    max relative error on species above atol <= 1e-3; against an FP64 oracle at rtol 1e-8
+    it may not be less accurate than the FP64 method by more than that margin."""
+    sub = {k: v[:1024] for k, v in cells4k.items()}
+    ierr, y64, _, rc, _, _ = run_gpu(sub, schedule=schedule)
+    assert ierr == 1
+    ierr, y32, st, _, ipar, _ = run_gpu(sub, precision=radm2b200.PREC_FP32LU, refine_sweeps=0, schedule=schedule)
+    assert ierr == 1 and (st["status"] == 1).all()
+    above = np.abs(y64) > 1.0
+    gate = np.abs(y32 - y64)[above] / np.abs(y64)[above]
+    assert gate.max() <= 1e-3
+    # no refinement: the float solves leave differences well above FP64 round-off
+    assert gate.max() > 1e-9
+    y_tight, _ = run_oracle(sub, rc, rtol=np.full(59, 1e-8))
+    above = np.abs(y_tight) > 1.0
+    e32 = np.abs(y32 - y_tight)[above] / np.abs(y_tight)[above]
+    e64 = np.abs(y64 - y_tight)[above] / np.abs(y_tight)[above]
+    assert e32.max() <= e64.max() + 1e-3
+    # one refinement sweep brings it back to FP64 round-off
+    _, y32r, _, _, _, _ = run_gpu(sub, precision=radm2b200.PREC_FP32LU, refine_sweeps=1, schedule=schedule)
+    g1 = np.abs(y32r - y64)[above] / np.maximum(np.abs(y64)[above], 1.0)
+    assert np.median(g1) <= 1e-12
+
+
 def test_kernel_timing_with_and_without_graph():
     """Solver-kernel timing works for host-driven splits and inside the split graph."""
     cells = inputs.make_cells(2048, 4, "plain", 0.3)
