@@ -124,9 +124,9 @@ inline int layout_check(int bs)
 #endif
 
 // ---------------------------------------------------------------- phases
-// Each phase is its own (non-inlined) function: the register allocator sees one
-// phase's live set at a time, and the RHS exists once in the instruction stream
-// although both Fcn0 and the stage-2 right-hand side use it.
+// Each phase is a function of its own, inlined into the kernel (RADM2_PHASE) except the
+// RHS (RADM2_FUN_PHASE), which exists once in the instruction stream although both Fcn0
+// and the stage-2 right-hand side use it.
 
 // dst = F(v): the RHS at state v (v and dst may alias; dst is written after v is read).
 template <int BS>
