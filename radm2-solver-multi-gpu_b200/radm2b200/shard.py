@@ -75,11 +75,13 @@ def gather_states(y_local, idx_local, ncell, dist=None, group=None):
     ibuf = torch.full((m,), -1, dtype=torch.int64)
     ybuf[:len(idx_local)] = torch.from_numpy(y_local)
     ibuf[:len(idx_local)] = torch.from_numpy(idx_local)
+    if dist.get_backend(group) == "nccl":  # NCCL moves device tensors only
+        ybuf, ibuf = ybuf.cuda(), ibuf.cuda()
     ys = [torch.empty_like(ybuf) for _ in range(world)]
     iss = [torch.empty_like(ibuf) for _ in range(world)]
     dist.all_gather(ys, ybuf, group=group)
     dist.all_gather(iss, ibuf, group=group)
     for r in range(world):
         k = sizes[r]
-        out[iss[r][:k].numpy()] = ys[r][:k].numpy()
+        out[iss[r][:k].cpu().numpy()] = ys[r][:k].cpu().numpy()
     return out
