@@ -59,6 +59,12 @@ typedef struct radm2_opts {
     int placement;      /* working-set placement: RADM2_PLACE_* (default GLOBAL) */
     int min_blocks;     /* register cap for occupancy: build variant with at least this many
                            resident blocks per SM (0/1 = no cap; 3 or 4 with 128 threads) */
+    int parity;         /* 1: reference-arithmetic FP64 solver -- the pivot divisions of
+                           dev_KppDecomp / dev_KppSolve (mgpu.cu:2766, 3086-3090) kept as
+                           divisions and no multiply-add contraction anywhere in the step, so
+                           every operation rounds as the reference's C expressions do
+                           (FP64 only; global placement; default 0 = the fast solver, which
+                           multiplies by reciprocal pivots and contracts multiply-adds) */
 } radm2_opts;
 
 /* Placement of each thread's working set (rate constants + state, and the LU). */
@@ -135,8 +141,10 @@ int radm2_set_rconst(radm2_ctx *ctx, const double *RCONST);
  * Integrate every cell from Tstart to Tend.  Replaces Rosenbrock() (mgpu.cu:3664-3848):
  * same IPAR/RPAR meaning and validation (IPAR[0] autonomous, IPAR[1] scalar tol,
  * IPAR[2] max steps, IPAR[3]=2 ROS-3; RPAR[0..6] Hmin, Hmax, Hstart, FacMin, FacMax,
- * FacRej, FacSafe), same return codes.  Counters are accumulated into IPAR[10..17]
- * (Nfun, Njac, Nstp, Nacc, Nrej, Ndec, Nsol, Nsng), summed over cells;
+ * FacRej, FacSafe), same return codes.  Counters are accumulated into IPAR[10..16]
+ * (Nfun, Njac, Nstp, Nacc, Nrej, Ndec, Nsol), summed over cells; each slot saturates at
+ * INT_MAX instead of wrapping (large batches exceed the int range: radm2_get_stats has
+ * the exact 64-bit totals); IPAR[17] (Nsng) is left as passed in.
  * RPAR[10] = Texit of the least advanced cell, RPAR[11] = smallest exit step.
  * Each cell runs its own step-size loop on the device; the call blocks until done.
  */
@@ -155,6 +163,14 @@ int radm2_run_split(radm2_ctx *ctx, int nsplit, double dt, const double *AbsTol,
  * rejected step counts, first accepted step size and exit step size. */
 int radm2_get_cell_stats(radm2_ctx *ctx, int *status, int *nacc, int *nrej, double *hfirst, double *hexit);
 int radm2_get_stats(radm2_ctx *ctx, radm2_stats *out);
+/* The IPAR statistics update every integration applies (the counter block of
+ * mgpu.cu:3835-3845): IPAR[10..16] += Nfun, Njac, Nstp, Nacc, Nrej, Ndec, Nsol of an
+ * integration with these 64-bit totals (Njac = accepted + failed cells' outer steps, Nfun
+ * adds one more per outer step when non-autonomous, Nsol = 3 per attempt), each slot
+ * saturating at INT_MAX.  Host only (no device needed), for callers that merge shards'
+ * totals into one IPAR. */
+int radm2_add_step_counters(int *IPAR, long long n_accepted, long long n_rejected, long long n_failed,
+                            int autonomous);
 
 /* Per-cell starting step override (device order = cell order), NULL clears it.
  * Values outside (0, Hmax] or non-finite fall back to the default Hstart. */
@@ -183,6 +199,10 @@ int radm2_decomp_solve(radm2_ctx *ctx, int n, int precision, double *G, double *
  * the summed device time (ms) and launch count since the previous call. */
 int radm2_set_kernel_timing(radm2_ctx *ctx, int enable);
 int radm2_get_kernel_time(radm2_ctx *ctx, double *ms, int *launches);
+/* Kernels one replay of the context's cached split graph launches (counted from the
+ * captured graph's kernel nodes; 0 when no graph is cached).  Every one is this library's
+ * own kernel.  No counterpart in the reference. */
+int radm2_get_graph_kernels(const radm2_ctx *ctx, int *kernels);
 
 /* Measured CUDA-core FMA throughput of a device (TFLOP/s, 2 flops per FMA): the
  * denominators of the solver's roofline.  Runs ~0.2 s of microbenchmark. */
@@ -308,11 +328,11 @@ int radm2_attach_mlp(radm2_ctx *ctx, radm2_mlp *mlp, int set_order);
 int radm2_selfcheck(void);
 
 /*
- * Integration without any device allocation, for callers that cannot call cudaMalloc:
- * code that runs while a CUDA graph is being captured (allocation fails under capture),
- * host frameworks that reserved all device memory for their own pool at start-up, and
- * real-time couplings whose memory budget is fixed at initialisation.  No counterpart in
- * the reference (which allocates inside Rosenbrock(), mgpu.cu:3444-3468).
+ * Integration without any device allocation, for callers that may not call cudaMalloc
+ * while they run: host frameworks that reserved all of the GPU's memory for their own pool
+ * at start-up (a later cudaMalloc fails or takes memory the pool counts on), and real-time
+ * or certified model couplings whose device memory budget is fixed at initialisation.  No
+ * counterpart in the reference (which allocates inside Rosenbrock(), mgpu.cu:3444-3468).
  *
  * Same method, IPAR/RPAR meaning and return codes as radm2_rosenbrock, but without a
  * context: inputs and outputs are the caller's device arrays in struct-of-arrays layout
@@ -323,10 +343,12 @@ int radm2_selfcheck(void);
  * in one statically sized device array of RADM2_NOALLOC_BYTES (64 MiB) that every GPU
  * which loads the library holds until the process exits.  Limits: ncell <= ld <=
  * RADM2_NOALLOC_MAX_CELLS; larger sizes return RADM2_E_TOOBIG (split the batch).
- * The first call on a device looks up the array's device address (set-up); make that
- * first call before any stream capture.  All calls share the array, so calls that
- * overlap on the GPU (other streams, other host threads) race: serialise them.  The
- * call blocks until the integration has finished.  Calls no allocating routine.
+ * Set-up: the first call on a device (and CUDA context) looks up the array's device
+ * address and loads the library's device code there.  All calls share the array, which
+ * keeps the previous call's contents (the call clears what must start at zero), so calls
+ * that overlap on the GPU (other streams, other host threads) race: serialise them.  The
+ * call waits for its stream before returning, as it reads the statistics back into
+ * IPAR/RPAR.  It calls no allocating routine.
  */
 #define RADM2_NOALLOC_MAX_CELLS 32768
 #define RADM2_NOALLOC_BYTES (64u << 20)

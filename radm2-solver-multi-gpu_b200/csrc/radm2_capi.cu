@@ -2,6 +2,7 @@
 // IPAR/RPAR parsing with the reference's checks, kernel launches and the
 // CUDA-graph operator-split loop.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -69,6 +70,22 @@ void drop_graph(radm2_ctx *c)
     if (c->gexec) cudaGraphExecDestroy(c->gexec);
     c->gexec = nullptr;
     c->gkey.clear();
+    c->graph_kernels = 0;
+}
+
+// Kernel nodes of a captured graph (memset, copy and event nodes are not counted).
+int count_kernel_nodes(cudaGraph_t g)
+{
+    size_t n = 0;
+    if (cudaGraphGetNodes(g, nullptr, &n) != cudaSuccess) return -1;
+    std::vector<cudaGraphNode_t> nodes(n);
+    if (n && cudaGraphGetNodes(g, nodes.data(), &n) != cudaSuccess) return -1;
+    int k = 0;
+    for (size_t i = 0; i < n; i++) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nodes[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) k++;
+    }
+    return k;
 }
 
 int ensure_cells(radm2_ctx *c, int ncell)
@@ -166,6 +183,20 @@ inline double absh(double x) { return (x >= 0) ? x : -x; }
 
 }  // namespace
 
+// IPAR[10..16] (Nfun, Njac, Nstp, Nacc, Nrej, Ndec, Nsol; mgpu.cu:3835-3845) from the 64-bit
+// totals of one integration.  Each slot saturates at INT_MAX instead of wrapping: the int
+// counters of the reference's interface overflow on large batches (3 solves per attempt over
+// 4M cells x 24 splits is ~2.4e9 solves).  radm2_stats keeps the exact 64-bit totals.
+void radm2::add_step_counters(int *IPAR, long long nacc, long long nrej, long long nfail, int autonomous)
+{
+    const long long natt = nacc + nrej, nouter = nacc + nfail;
+    const long long add[7] = {nouter * (autonomous ? 1 : 2) + natt, nouter, natt, nacc, nrej, natt, 3 * natt};
+    for (int k = 0; k < 7; k++) {
+        const long long v = (long long)IPAR[10 + k] + add[k];
+        IPAR[10 + k] = v > INT_MAX ? INT_MAX : (v < INT_MIN ? INT_MIN : (int)v);
+    }
+}
+
 // IPAR/RPAR parsing and validation, mgpu.cu:3684-3811 (same checks, same order, same codes).
 int radm2::parse_params(double Tstart, double Tend, const double *AbsTol, const double *RelTol, const double *RPAR,
                  const int *IPAR, int float_coeffs, SolveParams *p, int *autonomous)
@@ -224,6 +255,7 @@ cudaError_t variant_info(radm2_ctx *c, int bs, SolverInfo *info)
     const bool fp32 = c->o.precision == RADM2_PREC_FP32LU;
     const bool pers = c->o.schedule == RADM2_SCHED_PERSISTENT;
     const int k = key_of(c, bs);
+    if (c->o.parity) return pers ? solver_info_fp64x_persistent(k, info) : solver_info_fp64x_static(k, info);
     if (fp32 && c->o.refine_sweeps == 0)
         return pers ? solver_info_fp32d_persistent(k, info) : solver_info_fp32d_static(k, info);
     if (fp32) return pers ? solver_info_fp32_persistent(k, info) : solver_info_fp32_static(k, info);
@@ -305,6 +337,8 @@ cudaError_t launch_solver(radm2_ctx *c, const SolveArgs &a, int bs, int grid)
     const bool fp32 = c->o.precision == RADM2_PREC_FP32LU;
     const bool pers = c->o.schedule == RADM2_SCHED_PERSISTENT;
     const int k = key_of(c, bs);
+    if (c->o.parity)  // reference arithmetic: divisions kept, no multiply-add contraction
+        return pers ? launch_solver_fp64x_persistent(a, k, grid, c->st) : launch_solver_fp64x_static(a, k, grid, c->st);
     if (fp32 && c->o.refine_sweeps == 0)  // the variants without the refinement code
         return pers ? launch_solver_fp32d_persistent(a, k, grid, c->st) : launch_solver_fp32d_static(a, k, grid, c->st);
     if (fp32)
@@ -386,15 +420,7 @@ int finish(radm2_ctx *c, int nres, int autonomous, double *RPAR, int *IPAR, int 
             hmin = r.hmin;
         }
     }
-    const long long natt = nacc + nrej;
-    const long long nouter = nacc + nfail;
-    IPAR[10] += (int)(nouter * (autonomous ? 1 : 2) + natt);  // Nfun
-    IPAR[11] += (int)nouter;                                   // Njac
-    IPAR[12] += (int)natt;                                     // Nstp
-    IPAR[13] += (int)nacc;                                     // Nacc
-    IPAR[14] += (int)nrej;                                     // Nrej
-    IPAR[15] += (int)natt;                                     // Ndec
-    IPAR[16] += (int)(3 * natt);                               // Nsol
+    add_step_counters(IPAR, nacc, nrej, nfail, autonomous);
     RPAR[10] = direction > 0 ? tmin : tmax;
     RPAR[11] = hmin;
     c->stats.n_accepted = nacc;
@@ -428,6 +454,7 @@ int radm2_opts_default(radm2_opts *o)
     o->float_coeffs = 1;
     o->placement = RADM2_PLACE_GLOBAL;
     o->min_blocks = 0;
+    o->parity = 0;
     return RADM2_OK;
 }
 
@@ -445,6 +472,8 @@ int radm2_create(radm2_ctx **out, const radm2_opts *opts)
     if (o.refine_sweeps < 0 || o.refine_sweeps > 2) return RADM2_E_ARG;
     if (o.placement != RADM2_PLACE_GLOBAL && o.placement != RADM2_PLACE_LU_SMEM && o.placement != RADM2_PLACE_ALL_SMEM)
         return RADM2_E_ARG;
+    if (o.parity != 0 && o.parity != 1) return RADM2_E_ARG;
+    if (o.parity && (o.precision != RADM2_PREC_FP64 || o.placement != RADM2_PLACE_GLOBAL)) return RADM2_E_ARG;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= o.device || o.device < 0) return RADM2_E_NODEV;
     cudaDeviceProp prop;
@@ -826,7 +855,7 @@ int radm2_run_split(radm2_ctx *c, int nsplit, double dt, const double *AbsTol, c
         const uintptr_t extra[9] = {(uintptr_t)nsplit,
                                     (uintptr_t)bs,
                                     (uintptr_t)grid,
-                                    (uintptr_t)((c->o.precision * 2 + c->o.schedule) * (1ull << 32) +
+                                    (uintptr_t)((c->o.parity * 4 + c->o.precision * 2 + c->o.schedule) * (1ull << 32) +
                                                 (unsigned)key_of(c, bs)),
                                     reinterpret_cast<uintptr_t>(c->mlp),
                                     (uintptr_t)mlp_generation(c->mlp),
@@ -849,6 +878,7 @@ int radm2_run_split(radm2_ctx *c, int nsplit, double dt, const double *AbsTol, c
             cudaError_t e = cudaStreamEndCapture(c->st, &g);
             if (rc) return rc;
             if (e != cudaSuccess) return fail_cuda(c, e, "cudaStreamEndCapture");
+            c->graph_kernels = count_kernel_nodes(g);
             e = cudaGraphInstantiate(&c->gexec, g, 0);
             cudaGraphDestroy(g);
             if (e != cudaSuccess) {
@@ -875,6 +905,13 @@ int radm2_get_cell_stats(radm2_ctx *c, int *status, int *nacc, int *nrej, double
     if (hfirst) CK(cudaMemcpyAsync(hfirst, c->hfirst, sizeof(double) * n, cudaMemcpyDeviceToHost, c->st));
     if (hexit) CK(cudaMemcpyAsync(hexit, c->hexit, sizeof(double) * n, cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
+    return RADM2_OK;
+}
+
+int radm2_add_step_counters(int *IPAR, long long n_accepted, long long n_rejected, long long n_failed, int autonomous)
+{
+    if (!IPAR || n_accepted < 0 || n_rejected < 0 || n_failed < 0) return RADM2_E_ARG;
+    add_step_counters(IPAR, n_accepted, n_rejected, n_failed, autonomous);
     return RADM2_OK;
 }
 
@@ -934,6 +971,13 @@ int radm2_set_kernel_timing(radm2_ctx *c, int enable)
     c->kernel_ms = 0.0;
     c->kernel_launches = 0;
     c->ev_used = 0;
+    return RADM2_OK;
+}
+
+int radm2_get_graph_kernels(const radm2_ctx *c, int *kernels)
+{
+    if (!valid_ctx(c) || !kernels) return RADM2_E_ARG;
+    *kernels = c->gexec ? c->graph_kernels : 0;
     return RADM2_OK;
 }
 
@@ -1039,7 +1083,9 @@ int radm2_autotune(radm2_ctx *c, double dt, const double *AbsTol, const double *
     std::vector<Cand> cands;
     for (int sched = RADM2_SCHED_STATIC; sched <= RADM2_SCHED_PERSISTENT; sched++) {
 #define RADM2_TUNE_CAND(BS_, PL_, MB_) cands.push_back({sched, BS_, PL_, MB_});
-        if (c->o.precision == RADM2_PREC_FP32LU) {
+        if (c->o.parity) {
+            RADM2_VARIANTS_FP64X(RADM2_TUNE_CAND)
+        } else if (c->o.precision == RADM2_PREC_FP32LU) {
             RADM2_VARIANTS_FP32(RADM2_TUNE_CAND)
         } else {
             RADM2_VARIANTS_FP64(RADM2_TUNE_CAND)
@@ -1188,11 +1234,15 @@ int radm2_selfcheck(void)
     // Layout bounds of every solver variant (host arithmetic only, no device needed).
     const int bad = solver_layout_check_fp64_static() | solver_layout_check_fp64_persistent() |
                     solver_layout_check_fp32_static() | solver_layout_check_fp32_persistent() |
-                    solver_layout_check_fp32d_static() | solver_layout_check_fp32d_persistent();
+                    solver_layout_check_fp32d_static() | solver_layout_check_fp32d_persistent() |
+                    solver_layout_check_fp64x_static() | solver_layout_check_fp64x_persistent();
     return bad ? RADM2_E_STATE : RADM2_OK;
 }
 
-const char *radm2_version(void) { return "radm2-b200 1.0 sm_100a (fp64 | fp32-LU+IR) x (static | persistent)"; }
+const char *radm2_version(void)
+{
+    return "radm2-b200 1.1 sm_100a (fp64 | fp64 reference arithmetic | fp32-LU+IR) x (static | persistent)";
+}
 
 // ---------------------------------------------------------------- mechanism kernels on host arrays
 

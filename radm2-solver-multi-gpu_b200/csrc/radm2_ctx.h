@@ -37,6 +37,7 @@ struct radm2_ctx {
     // cached split graph
     cudaGraphExec_t gexec = nullptr;
     std::vector<unsigned char> gkey;
+    int graph_kernels = 0;  // kernel nodes of the cached split graph
     // solver-kernel timing
     bool timing = false;
     std::vector<cudaEvent_t> ev;  // start/stop pairs, one per result slot

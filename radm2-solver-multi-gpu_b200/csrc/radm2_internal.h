@@ -21,6 +21,9 @@ struct RunResult {
 int parse_params(double Tstart, double Tend, const double *AbsTol, const double *RelTol, const double *RPAR,
                  const int *IPAR, int float_coeffs, SolveParams *p, int *autonomous);
 
+// Add one integration's 64-bit step totals to IPAR[10..16], saturating at INT_MAX.
+void add_step_counters(int *IPAR, long long nacc, long long nrej, long long nfail, int autonomous);
+
 cudaError_t launch_rconst(int n, int ld, const double *jv, const double *temp, const double *fix,
                           const double *rcn2o5, double *rconst, cudaStream_t st);
 cudaError_t launch_aos_to_soa(int n, int m, int ld, const double *aos, double *soa, cudaStream_t st);
@@ -50,6 +53,8 @@ cudaError_t launch_reduce(int n, const int *status, const int *nacc, const int *
 // registers per thread (65536 / (bs * minb)) for occupancy.
 #define RADM2_VARIANTS_FP64(X) X(32, 0, 1) X(64, 0, 1) X(128, 0, 1) X(256, 0, 1) X(128, 0, 3) X(128, 0, 4) X(32, 1, 1) X(32, 3, 1)
 #define RADM2_VARIANTS_FP32(X) X(64, 0, 1) X(128, 0, 1) X(256, 0, 1) X(128, 0, 3) X(128, 0, 4) X(32, 1, 1) X(64, 1, 1) X(32, 3, 1)
+// Reference-arithmetic FP64 solver (radm2_opts.parity): global placement only.
+#define RADM2_VARIANTS_FP64X(X) X(32, 0, 1) X(64, 0, 1) X(128, 0, 1) X(256, 0, 1)
 
 // Static properties of one solver variant on the current device.
 struct SolverInfo {
@@ -71,12 +76,17 @@ cudaError_t launch_solver_fp32_persistent(const SolveArgs &a, int key, int grid,
 // FP32 LU without the refinement code (refine_sweeps = 0); same variant keys as fp32.
 cudaError_t launch_solver_fp32d_static(const SolveArgs &a, int key, int grid, cudaStream_t st);
 cudaError_t launch_solver_fp32d_persistent(const SolveArgs &a, int key, int grid, cudaStream_t st);
+// Reference-arithmetic FP64 (divisions kept, no multiply-add contraction); FP64 variant keys.
+cudaError_t launch_solver_fp64x_static(const SolveArgs &a, int key, int grid, cudaStream_t st);
+cudaError_t launch_solver_fp64x_persistent(const SolveArgs &a, int key, int grid, cudaStream_t st);
 cudaError_t solver_info_fp64_static(int key, SolverInfo *out);
 cudaError_t solver_info_fp64_persistent(int key, SolverInfo *out);
 cudaError_t solver_info_fp32_static(int key, SolverInfo *out);
 cudaError_t solver_info_fp32_persistent(int key, SolverInfo *out);
 cudaError_t solver_info_fp32d_static(int key, SolverInfo *out);
 cudaError_t solver_info_fp32d_persistent(int key, SolverInfo *out);
+cudaError_t solver_info_fp64x_static(int key, SolverInfo *out);
+cudaError_t solver_info_fp64x_persistent(int key, SolverInfo *out);
 // Host-side bounds check of every built variant's working-set layout (0 = all in bounds).
 int solver_layout_check_fp64_static();
 int solver_layout_check_fp64_persistent();
@@ -84,5 +94,7 @@ int solver_layout_check_fp32_static();
 int solver_layout_check_fp32_persistent();
 int solver_layout_check_fp32d_static();
 int solver_layout_check_fp32d_persistent();
+int solver_layout_check_fp64x_static();
+int solver_layout_check_fp64x_persistent();
 
 }  // namespace radm2

@@ -1,20 +1,21 @@
 // radm2_rosenbrock_noalloc: the integration for callers that cannot allocate device
 // memory.
 //
-// Some callers may not call cudaMalloc at all: code that runs while a CUDA graph is being
-// captured (allocation is not a stream operation and fails under capture), host
-// frameworks that reserved all device memory for their own pool at start-up, and
-// real-time couplings whose memory budget is fixed at initialisation.  This entry point
-// takes device pointers for the inputs and outputs and keeps everything else it needs
-// -- the solver kernel's per-thread scratch slots, the rate-constant table and the
-// per-cell bookkeeping -- in one statically sized array in this file.  It runs the same
-// rate-constant, solver and reduction kernels as radm2_rosenbrock (the solver with the
-// working set of each cell in shared memory, so its global scratch is small).
+// Some callers may not call cudaMalloc while they run: a host framework that reserved all
+// of the GPU's memory for its own pool at start-up (a later cudaMalloc fails or steals from
+// that pool), and real-time or certified couplings whose device memory budget is fixed at
+// initialisation and may not grow once the model is running.  This entry point takes device
+// pointers for the inputs and outputs and keeps everything else it needs -- the solver
+// kernel's per-thread scratch slots, the rate-constant table and the per-cell bookkeeping --
+// in one statically sized array in this file.  It runs the same rate-constant, solver and
+// reduction kernels as radm2_rosenbrock (the solver with the working set of each cell in
+// shared memory, so its global scratch is small).
 //
 // The array is a __device__ object: every GPU that loads the library holds its
 // RADM2_NOALLOC_BYTES until the process exits.  Host code cannot use the array's name as
-// a device address, so the address is fetched with cudaGetSymbolAddress once per device
-// (on that device's first call, with the device current) and passed to the kernels.
+// a device address (in host code it names a host-side stand-in), so the address is
+// fetched with cudaGetSymbolAddress on the first call made with a given device and CUDA
+// context current, and passed to the kernels.
 #include <cstring>
 #include <mutex>
 
@@ -53,19 +54,47 @@ static_assert(kTotal <= (size_t)RADM2_NOALLOC_BYTES, "no-alloc area larger than 
 __device__ __align__(256) unsigned char g_noalloc_area[RADM2_NOALLOC_BYTES];
 
 std::mutex g_setup_mutex;
-void *g_area_addr[256];  // per-device address of g_noalloc_area, filled on first use
+// Per device: the CUDA context the address was looked up in, and the address.  A device
+// reset (cudaDeviceReset) or a new primary context reloads the module at a new address, so
+// the cached address is only reused while the same context is current.
+struct AreaSlot {
+    void *ctx;
+    void *addr;
+};
+AreaSlot g_area[256];
 
-// Device address of the area on the current device (set-up on the first call per device).
+using CtxGetCurrentFn = int (*)(void **);
+CtxGetCurrentFn ctx_get_current()
+{
+    static CtxGetCurrentFn fn = [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return reinterpret_cast<CtxGetCurrentFn>(f);
+    }();
+    return fn;
+}
+
+// Device address of the area on the current device and context (set-up on the first call
+// with that pair current; without the context query, looked up on every call).
 cudaError_t area_address(int device, unsigned char **out)
 {
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_area_addr[device]) {
+    void *ctx = nullptr;
+    CtxGetCurrentFn get = ctx_get_current();
+    const bool known_ctx = get && get(&ctx) == 0 && ctx;
+    if (!known_ctx || !g_area[device].addr || g_area[device].ctx != ctx) {
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_area);
         if (e != cudaSuccess) return e;
-        g_area_addr[device] = p;
+        g_area[device].ctx = known_ctx ? ctx : nullptr;
+        g_area[device].addr = known_ctx ? p : nullptr;
+        *out = static_cast<unsigned char *>(p);
+        return cudaSuccess;
     }
-    *out = static_cast<unsigned char *>(g_area_addr[device]);
+    *out = static_cast<unsigned char *>(g_area[device].addr);
     return cudaSuccess;
 }
 
@@ -135,14 +164,7 @@ extern "C" int radm2_rosenbrock_noalloc(int ncell, int ld, double *var, const do
         cudaStreamSynchronize(st) != cudaSuccess)
         return RADM2_E_CUDA;
 
-    const long long natt = r.nacc + r.nrej, nouter = r.nacc + r.nfail;
-    IPAR[10] += (int)(nouter * (autonomous ? 1 : 2) + natt);
-    IPAR[11] += (int)nouter;
-    IPAR[12] += (int)natt;
-    IPAR[13] += (int)r.nacc;
-    IPAR[14] += (int)r.nrej;
-    IPAR[15] += (int)natt;
-    IPAR[16] += (int)(3 * natt);
+    add_step_counters(IPAR, r.nacc, r.nrej, r.nfail, autonomous);
     RPAR[10] = p.direction > 0 ? r.tmin : r.tmax;
     RPAR[11] = r.hmin;
     return r.worst;

@@ -269,23 +269,6 @@ __device__ RADM2_PHASE void ph_stage(int stage, const double *y, const double *r
 #undef G
 }
 
-// Optional per-phase cycle counters (build with -DRADM2_PHASE_CLOCKS): lane 0 of every
-// warp adds clock64() deltas per phase into phase_clocks[warp][8]; profiling only.
-#ifdef RADM2_PHASE_CLOCKS
-__device__ unsigned long long phase_clocks[1 << 16][8];
-#define PCLK_DECL long long pclk_t = clock64();
-#define PCLK(ph)                                                                                   \
-    do {                                                                                           \
-        const long long t_ = clock64();                                                            \
-        if ((threadIdx.x & 31) == 0)                                                               \
-            phase_clocks[(blockIdx.x * BS + threadIdx.x) >> 5 & 0xffff][ph] += (unsigned long long)(t_ - pclk_t); \
-        pclk_t = t_;                                                                               \
-    } while (0)
-#else
-#define PCLK_DECL
-#define PCLK(ph) do { } while (0)
-#endif
-
 template <int BS, typename LUT, int SCHED, int PLACE, int MINB, int IR = 1>
 __global__ void __launch_bounds__(BS, MINB) k_rosenbrock(const SolveArgs a)
 {
@@ -375,7 +358,6 @@ __global__ void __launch_bounds__(BS, MINB) k_rosenbrock(const SolveArgs a)
     };
 
     if (have) load_cell(cell);
-    PCLK_DECL
 
     for (;;) {
         // Bring every lane that still has work to the start of a step attempt.
@@ -397,7 +379,6 @@ __global__ void __launch_bounds__(BS, MINB) k_rosenbrock(const SolveArgs a)
             ph_fun<BS>(rcy + RCY_Y * BS, rcy + RCY_RC * BS, vec + VEC_F0 * BS, fix0, fix1);
             outer = false;
         }
-        PCLK(0);  // outer: cell load/store, time-loop test, Fcn0
         if (!__any_sync(0xffffffffu, have)) break;
         if (!have) continue;
 
@@ -415,9 +396,7 @@ __global__ void __launch_bounds__(BS, MINB) k_rosenbrock(const SolveArgs a)
         const double ghinv = 1.0 / (dir * H * RADM2_ROS_GAMMA0);
         // G = -J(Y) + ghinv I, written straight into the LU slots; then factor it.
         ph_jac<BS, LUT>(rcy + RCY_Y * BS, rcy + RCY_RC * BS, sg, fix0, fix1, ghinv);
-        PCLK(1);
         const int sing = ph_decomp<BS, LUT>(sg);
-        PCLK(2);
         if (sing) {
             status = -8;
             done = true;
@@ -431,7 +410,6 @@ __global__ void __launch_bounds__(BS, MINB) k_rosenbrock(const SolveArgs a)
         for (int stage = 0; stage < 3; stage++) {
             ph_stage<BS, LUT, IR>(stage, rcy + RCY_Y * BS, rcy + RCY_RC * BS, vec, sg, fix0, fix1, hc21, hc31, hc32, ghinv,
                               a.refine);
-            PCLK(3 + stage);
         }
         nstp++;
 
@@ -474,7 +452,6 @@ __global__ void __launch_bounds__(BS, MINB) k_rosenbrock(const SolveArgs a)
             nrej++;
             H = hnew;
         }
-        PCLK(6);  // error norm and step control
     }
 #undef RW
 #undef VW

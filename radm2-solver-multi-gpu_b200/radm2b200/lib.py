@@ -32,7 +32,8 @@ NFEAT = 84
 class Opts(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("precision", ctypes.c_int), ("refine_sweeps", ctypes.c_int),
                 ("schedule", ctypes.c_int), ("block_threads", ctypes.c_int), ("blocks_per_sm", ctypes.c_int),
-                ("float_coeffs", ctypes.c_int), ("placement", ctypes.c_int), ("min_blocks", ctypes.c_int)]
+                ("float_coeffs", ctypes.c_int), ("placement", ctypes.c_int), ("min_blocks", ctypes.c_int),
+                ("parity", ctypes.c_int)]
 
 
 class WrfGrid(ctypes.Structure):
@@ -74,6 +75,8 @@ SIGNATURES = {
                                        ctypes.c_int]),
     "radm2_get_cell_stats": (ctypes.c_int, [ctypes.c_void_p, _I, _I, _I, _D, _D]),
     "radm2_get_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Stats)]),
+    "radm2_add_step_counters": (ctypes.c_int, [_I, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_longlong,
+                                               ctypes.c_int]),
     "radm2_set_cell_hstart": (ctypes.c_int, [ctypes.c_void_p, _D]),
     "radm2_set_cell_order": (ctypes.c_int, [ctypes.c_void_p, _I]),
     "radm2_fun": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _D, _D, _D, _D]),
@@ -81,6 +84,7 @@ SIGNATURES = {
     "radm2_decomp_solve": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _D, _D, _I]),
     "radm2_set_kernel_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "radm2_get_kernel_time": (ctypes.c_int, [ctypes.c_void_p, _D, _I]),
+    "radm2_get_graph_kernels": (ctypes.c_int, [ctypes.c_void_p, _I]),
     "radm2_fma_peak": (ctypes.c_int, [ctypes.c_int, _D, _D]),
     "radm2_mlp_nparams": (ctypes.c_int, []),
     "radm2_mlp_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_uint]),
@@ -172,6 +176,18 @@ class RadmError(RuntimeError):
         self.code = code
 
 
+def add_step_counters(ipar, n_accepted, n_rejected, n_failed=0, autonomous=True):
+    """IPAR[10..16] += the statistics of an integration with these 64-bit step totals, each
+    slot saturating at INT_MAX (the library's own update; no device needed)."""
+    lib = load()
+    assert ipar.dtype == np.int32 and ipar.flags.c_contiguous
+    rc = lib.radm2_add_step_counters(_ip(ipar), int(n_accepted), int(n_rejected), int(n_failed),
+                                     1 if autonomous else 0)
+    if rc != 0:
+        raise RadmError(rc, lib.radm2_error_string(rc).decode())
+    return ipar
+
+
 def default_params(hstart=0.0, max_steps=0, autonomous=True):
     """IPAR/RPAR as the reference driver sets them (mgpu.cu:3863-3873)."""
     ipar = np.zeros(20, dtype=np.int32)
@@ -187,7 +203,7 @@ class Solver:
     """One device context of the batched solver."""
 
     def __init__(self, precision=PREC_FP64, schedule=SCHED_STATIC, refine_sweeps=1, block_threads=0,
-                 blocks_per_sm=0, float_coeffs=1, device=0, placement=PLACE_GLOBAL, min_blocks=0):
+                 blocks_per_sm=0, float_coeffs=1, device=0, placement=PLACE_GLOBAL, min_blocks=0, parity=0):
         self.lib = load()
         o = Opts()
         self.lib.radm2_opts_default(ctypes.byref(o))
@@ -195,6 +211,7 @@ class Solver:
         o.block_threads, o.blocks_per_sm, o.float_coeffs = block_threads, blocks_per_sm, float_coeffs
         o.placement = placement
         o.min_blocks = min_blocks
+        o.parity = parity
         h = ctypes.c_void_p()
         rc = self.lib.radm2_create(ctypes.byref(h), ctypes.byref(o))
         if rc != 0:
@@ -318,6 +335,12 @@ class Solver:
         ms, n = ctypes.c_double(), ctypes.c_int()
         self._check(self.lib.radm2_get_kernel_time(self.h, ctypes.byref(ms), ctypes.byref(n)))
         return ms.value, n.value
+
+    def graph_kernels(self):
+        """Kernel nodes of the cached split graph (kernels per replay; 0 = none cached)."""
+        n = ctypes.c_int()
+        self._check(self.lib.radm2_get_graph_kernels(self.h, ctypes.byref(n)))
+        return n.value
 
     def device_bytes(self):
         return int(self.lib.radm2_device_bytes(self.h))

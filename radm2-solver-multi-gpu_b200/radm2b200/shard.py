@@ -44,16 +44,32 @@ def balanced_assignment(costs, world):
     return [np.sort(order[rank == r]) for r in range(world)]
 
 
-def reduce_counters(ipar, dist=None, group=None):
-    """Sum the counter slots of IPAR over ranks (in place); other slots are untouched."""
+INT_MAX = 2 ** 31 - 1
+
+
+def reduce_totals(values, dist=None, group=None):
+    """Sum 64-bit totals (e.g. radm2_stats' accepted/rejected step counts) over ranks;
+    returns a list of Python ints on every rank."""
+    vals = [int(v) for v in values]
     if dist is None or not dist.is_initialized() or dist.get_world_size(group) == 1:
-        return ipar
+        return vals
     import torch
-    t = torch.tensor(np.asarray(ipar[IPAR_COUNTERS], dtype=np.int64))
+    t = torch.tensor(vals, dtype=torch.int64)
     if dist.get_backend(group) == "nccl":
         t = t.cuda()
     dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
-    ipar[IPAR_COUNTERS] = t.cpu().numpy().astype(ipar.dtype)
+    return [int(x) for x in t.cpu().tolist()]
+
+
+def reduce_counters(ipar, dist=None, group=None):
+    """Sum the counter slots of IPAR over ranks (in place), in 64-bit arithmetic, each slot
+    saturating at INT_MAX as the library's own update does (int IPAR slots cannot hold the
+    sums of large multi-GPU runs; reduce_totals over radm2_stats gives the exact totals).
+    Other slots are untouched."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size(group) == 1:
+        return ipar
+    summed = reduce_totals(np.asarray(ipar[IPAR_COUNTERS], dtype=np.int64), dist, group)
+    ipar[IPAR_COUNTERS] = np.minimum(np.asarray(summed, dtype=np.int64), INT_MAX).astype(ipar.dtype)
     return ipar
 
 

@@ -330,14 +330,12 @@ def test_tiny_and_odd_batches_match_oracle(n):
     assert rel_err(ys[0], y_o).max() <= PARITY
 
 
-def test_mixed_regime_parity():
-    """The 1e-10 parity bar is set on the plain workload.  On the mixed-regime batch (urban
-    NOx, 220 K) the solver's fused multiply-adds and reciprocal pivots, against the oracle's
-    unfused divisions, move a few stiff cells' species near atol by up to a few 1e-10
-    relative; step counts stay identical."""
+def _mixed_case(**opts):
+    """The 4,096-cell mixed-regime batch (urban NOx, 220 K) on the GPU and the oracle, both
+    fed the GPU's rate constants: per-element errors and both sets of cell statistics."""
     cells = inputs.make_cells(4096, 23, "mixed")
     atol, rtol = np.ones(59), np.full(59, 1e-3)
-    with radm2b200.Solver(schedule=radm2b200.SCHED_PERSISTENT) as s:
+    with radm2b200.Solver(schedule=radm2b200.SCHED_PERSISTENT, **opts) as s:
         s.set_cells(cells)
         s.update_rconst()
         rc = s.get_rconst()
@@ -348,11 +346,90 @@ def test_mixed_regime_parity():
     ipar, rpar = radm2b200.default_params(hstart=6.0)
     ok, p = oracle.params(0.0, 600.0, atol, rtol, rpar, ipar)
     y_o, st_o = oracle.integrate(cells["VAR"], cells["FIX"], rc, p)
-    e = rel_err(y, y_o)
-    print("mixed parity: max %.2e, cells above 1e-10: %d, above 1e-12: %d"
+    return rel_err(y, y_o), st, st_o
+
+
+def test_mixed_regime_parity():
+    """Reference arithmetic (radm2_opts.parity: pivot divisions kept, no multiply-add
+    contraction) on the mixed-regime batch: within 1e-10 of the oracle, identical step counts."""
+    e, st, st_o = _mixed_case(parity=1)
+    print("mixed parity (reference arithmetic): max %.2e" % e.max())
+    assert np.array_equal(st["nacc"], st_o["nacc"]) and np.array_equal(st["nrej"], st_o["nrej"])
+    assert e.max() <= PARITY
+
+
+def test_mixed_regime_fast_solver_deviation():
+    """The fast solver (reciprocal pivots, contracted multiply-adds) on the same batch: its
+    deviation from the oracle is reported; step counts stay identical.  Measured 2.0e-10 on
+    B200 (a few stiff cells' species near atol)."""
+    e, st, st_o = _mixed_case()
+    print("mixed parity (fast solver): max %.2e, cells above 1e-10: %d, above 1e-12: %d"
           % (e.max(), int((e.max(1) > 1e-10).sum()), int((e.max(1) > 1e-12).sum())))
     assert np.array_equal(st["nacc"], st_o["nacc"]) and np.array_equal(st["nrej"], st_o["nrej"])
     assert e.max() <= 1e-9
+
+
+def _six_splits(parity):
+    """configs[1]'s hour as 6 consecutive 600 s operator splits (Hstart 0.01 dt, the state
+    carried over) on every 256th cell of the 1,048,576-cell, 30%-night workload (4,096
+    cells): the GPU one split at a time, the oracle likewise, compared after every split."""
+    n, seed, wl, night, _ = inputs.WORKLOADS["plain-1m"]
+    idx = np.arange(0, n, 256)
+    cells = inputs.make_cells(n, seed, wl, night)
+    sub = {k: np.ascontiguousarray(v[idx]) for k, v in cells.items()}
+    atol, rtol = np.ones(59), np.full(59, 1e-3)
+    worst, per_split = 0.0, []
+    with radm2b200.Solver(schedule=radm2b200.SCHED_PERSISTENT, parity=parity) as s:
+        s.set_cells(sub)
+        s.update_rconst()
+        rc = s.get_rconst()
+        ipar, rpar = radm2b200.default_params(hstart=6.0)
+        ok, p = oracle.params(0.0, 600.0, atol, rtol, rpar, ipar)
+        y_o = sub["VAR"]
+        for k in range(6):
+            ipar, rpar = radm2b200.default_params()
+            assert s.run_split(1, 600.0, atol, rtol, rpar, ipar) == 1
+            y, st = s.get_state(), s.cell_stats()
+            y_o, st_o = oracle.integrate(y_o, sub["FIX"], rc, p)
+            same_steps = np.array_equal(st["nacc"], st_o["nacc"]) and np.array_equal(st["nrej"], st_o["nrej"])
+            e = rel_err(y, y_o).max()
+            worst = max(worst, e)
+            per_split.append((k, e, same_steps))
+        y_seq = s.get_state()
+    # the same hour as one 6-split graph from the initial state ends in the same state
+    with radm2b200.Solver(schedule=radm2b200.SCHED_PERSISTENT, parity=parity) as s:
+        s.set_cells(sub)
+        ipar, rpar = radm2b200.default_params()
+        assert s.run_split(6, 600.0, atol, rtol, rpar, ipar) == 1
+        assert np.array_equal(s.get_state(), y_seq)
+    return worst, per_split
+
+
+def test_six_split_hour_parity():
+    """Reference arithmetic over 6 consecutive splits: within 1e-10 of the oracle after every
+    split, with identical per-cell accepted and rejected step counts in every split."""
+    worst, per_split = _six_splits(1)
+    print("6-split parity (reference arithmetic):", ["%d: %.2e" % (k, e) for k, e, _ in per_split])
+    assert all(same for _, _, same in per_split), per_split
+    assert worst <= PARITY
+
+
+def test_six_split_hour_fast_solver_deviation():
+    """The fast solver over the same 6 splits: its largest deviation from the oracle is
+    reported (the states and the step counts are compared after every split)."""
+    worst, per_split = _six_splits(0)
+    print("6-split deviation (fast solver):", ["%d: %.2e steps %s" % x for x in per_split])
+    assert worst <= 1e-8
+
+
+def test_parity_option_validation():
+    """The reference-arithmetic solver exists for FP64 with global placement only."""
+    with pytest.raises(radm2b200.RadmError):
+        radm2b200.Solver(parity=1, precision=radm2b200.PREC_FP32LU)
+    with pytest.raises(radm2b200.RadmError):
+        radm2b200.Solver(parity=1, placement=radm2b200.lib.PLACE_LU_SMEM)
+    with radm2b200.Solver(parity=1) as s:
+        assert s.opts()["parity"] == 1
 
 
 def _parity_case(sub, tstart, tend, atol, rtol, ipar, rpar):

@@ -47,3 +47,26 @@ def test_parameter_validation_codes():
     assert _code(atol=0.0) == -5                  # AbsTol <= 0
     assert _code(rtol=1.0) == -5                  # RelTol >= 1
     assert _code(rtol=1e-20) == -5                # RelTol <= 10 * roundoff
+
+
+def test_step_counters_saturate_instead_of_wrapping():
+    """IPAR[10..16] are C ints in the reference's interface.  A 4M-cell, 24-split batch takes
+    ~0.8e9 step attempts, so Nsol (3 per attempt) passes 2^31: the library's update (the one
+    radm2_rosenbrock applies, called here on the host) saturates each slot at INT_MAX."""
+    big = 10 ** 9
+    ipar = np.zeros(20, dtype=np.int32)
+    radm2b200.add_step_counters(ipar, big, 5, n_failed=2)
+    assert ipar[13] == big and ipar[14] == 5
+    assert ipar[12] == big + 5 and ipar[15] == big + 5      # Nstp, Ndec
+    assert ipar[11] == big + 2                              # Njac: accepted + failed outer steps
+    assert ipar[10] == (big + 2) + (big + 5)                # Nfun, autonomous
+    assert ipar[16] == 2 ** 31 - 1                          # Nsol = 3 x 1e9 + 15: saturated
+    radm2b200.add_step_counters(ipar, big, 0)               # a second integration
+    assert ipar[13] == 2 * big and ipar[10] == 2 ** 31 - 1 and ipar[16] == 2 ** 31 - 1
+    radm2b200.add_step_counters(ipar, big, 0)
+    assert ipar[13] == 2 ** 31 - 1 and (ipar[10:17] > 0).all()  # never wraps negative
+    assert ipar[17] == 0 and ipar[:10].sum() == 0
+    # small counts add exactly, as before
+    ipar = np.zeros(20, dtype=np.int32)
+    radm2b200.add_step_counters(ipar, 7, 3, autonomous=False)
+    assert list(ipar[10:17]) == [2 * 7 + 10, 7, 10, 7, 3, 10, 30]

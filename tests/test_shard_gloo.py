@@ -84,3 +84,31 @@ def test_two_rank_integration_equals_one_process(tmp_path):
     y, st = oracle.integrate(cells["VAR"], cells["FIX"], rc, p, 1)
     assert np.array_equal(got["y"], y)
     assert int(got["ipar"][13]) == int(np.sum(st["nacc"])) and int(got["ipar"][14]) == int(np.sum(st["nrej"]))
+
+
+def _counter_rank(rank, world, port, out_path):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    # each rank's counters fit an int; their sum over ranks does not
+    ip = np.zeros(20, dtype=np.int32)
+    ip[13], ip[14], ip[16] = 1_500_000_000, 40_000_000 + rank, 2_000_000_000
+    shard.reduce_counters(ip, dist)
+    tot = shard.reduce_totals([1_500_000_000, 40_000_000 + rank], dist)
+    if rank == 0:
+        np.savez(out_path, ipar=ip, tot=np.array(tot, dtype=np.int64))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_counters_summed_over_ranks_beyond_int32(tmp_path):
+    """Two ranks whose summed step counters exceed 2^31: the IPAR slots saturate at INT_MAX
+    (as the library's own update does) instead of wrapping, and the 64-bit totals the
+    benchmark uses come back exact."""
+    out = str(tmp_path / "c.npz")
+    mp.start_processes(_counter_rank, args=(2, _free_port(), out), nprocs=2, start_method="spawn", join=True)
+    got = np.load(out)
+    assert int(got["ipar"][13]) == 2 ** 31 - 1 and int(got["ipar"][16]) == 2 ** 31 - 1
+    assert int(got["ipar"][14]) == 80_000_001
+    assert list(got["tot"]) == [3_000_000_000, 80_000_001]
