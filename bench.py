@@ -58,6 +58,7 @@ WORKLOADS = {
     "mixed-256k": (262144, 3, "mixed", 0.4, 600.0),      # quick check of the default path
 }
 ATOL, RTOL, RTOL_TIGHT = 1.0, 1.0e-3, 1.0e-8
+SCHED_NAMES = {0: "static", 1: "persistent", 2: "coop"}
 
 
 # HBM copy bandwidth of a B200 when no measured peak file is present (GB/s).
@@ -73,7 +74,8 @@ def parse():
     ap.add_argument("--workload", default="mixed-4m-eval", choices=sorted(WORKLOADS))
     ap.add_argument("--method", default="learned", choices=["learned", "plain"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32lu"])
-    ap.add_argument("--schedule", default="persistent", choices=["static", "persistent"])
+    ap.add_argument("--schedule", default="persistent", choices=["static", "persistent", "coop"],
+                    help="starting schedule (the autotuner may pick another); coop = cooperative blocks")
     ap.add_argument("--refine", type=int, default=1, choices=[0, 1, 2],
                     help="fp32lu: FP64 refinement sweeps per stage solve")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shape")
@@ -254,6 +256,16 @@ def per_species_errors(y, ref):
     return out
 
 
+def solver_kernel_name(tuned, args):
+    """The solver kernel the timed arm launched (after autotuning, if any)."""
+    sched, bs = args.schedule, args.block_threads
+    if tuned is not None:
+        sched, bs = SCHED_NAMES[tuned["chosen"]["schedule"]], tuned["chosen"]["block_threads"]
+    if sched == "coop":
+        return "k_rosenbrock_coop%s_g%d (cooperative solver)" % ("x" if args.parity else "", (bs or 256) // 32)
+    return "k_rosenbrock (thread-per-cell solver, %s)" % sched
+
+
 def rel_errors(y, ref):
     """Relative errors of y against ref on entries above atol, and on entries where the
     relative tolerance governs the error control (|ref| >= atol / rtol)."""
@@ -288,7 +300,8 @@ def main():
     learned = args.method == "learned"
     cells = inputs.make_cells(ncell, seed, wl, night, first_cell=rank * ncell)
     prec = radm2b200.PREC_FP32LU if args.precision == "fp32lu" else radm2b200.PREC_FP64
-    sched = radm2b200.SCHED_PERSISTENT if args.schedule == "persistent" else radm2b200.SCHED_STATIC
+    sched = {"static": radm2b200.SCHED_STATIC, "persistent": radm2b200.SCHED_PERSISTENT,
+             "coop": radm2b200.SCHED_COOP}[args.schedule]
     refine = args.refine
     atol, rtol = np.full(59, ATOL), np.full(59, RTOL)
     stream = torch.cuda.Stream()
@@ -535,7 +548,7 @@ def main():
             tr = json.load(f)
         sched_used = args.schedule
         if main_arm["tuned"] is not None:
-            sched_used = "persistent" if main_arm["tuned"]["chosen"]["schedule"] else "static"
+            sched_used = SCHED_NAMES[main_arm["tuned"]["chosen"]["schedule"]]
         key = "%s-%s" % (args.precision, sched_used)
         if key + "-" + wl in tr:  # a capture of this workload family, if there is one
             key = key + "-" + wl
@@ -584,7 +597,7 @@ def main():
                      "frac": (achieved / fp64_peak) if achieved else None, "traffic": traffic,
                      "peak_source": "measured CUDA-core FP64 FMA microbenchmark (radm2_fma_peak); FP32 %.1f"
                                     % fp32_peak,
-                     "kernel": "k_rosenbrock (solver)",
+                     "kernel": solver_kernel_name(main_arm["tuned"], args),
                      "kernel_ms_per_launch": kms / max(klaunch, 1), "flops_per_launch": per_launch_flops,
                      "traffic_gbs": traffic_gbs, "traffic_capture": traffic_src,
                      "traffic_frac_of_hbm": (traffic_gbs / hbm) if (traffic_gbs and hbm) else None,
@@ -597,7 +610,7 @@ def main():
     if main_arm["tuned"] is not None:
         line["autotune"] = main_arm["tuned"]
         ch = main_arm["tuned"]["chosen"]
-        line["config"]["schedule"] = "persistent" if ch["schedule"] else "static"
+        line["config"]["schedule"] = SCHED_NAMES[ch["schedule"]]
         line["config"]["launch"] = "%d threads/block, placement %d, min blocks %d (autotuned)" % (
             ch["block_threads"], ch["placement"], ch["min_blocks"])
     if train is not None:

@@ -47,13 +47,19 @@ extern "C" {
 
 #define RADM2_SCHED_STATIC 0     /* one thread per cell, cells in order (plain) */
 #define RADM2_SCHED_PERSISTENT 1 /* persistent grid, per-lane work stealing */
+#define RADM2_SCHED_COOP 2       /* cooperative: 32 cells per block with the whole working set
+                                    (LU, state, stage vectors) on chip; the block's warps split
+                                    every phase of a step between them, so each cell is served
+                                    by one lane in each warp; block_threads 128 (4 warps per cell
+                                    group) or 256 (8, default); FP64; cells from a work queue */
 
 typedef struct radm2_opts {
     int device;         /* CUDA device ordinal (default 0) */
     int precision;      /* RADM2_PREC_* (default FP64) */
     int refine_sweeps;  /* FP32LU: FP64 refinement sweeps per stage solve, 0..2 (default 1) */
     int schedule;       /* RADM2_SCHED_* (default STATIC) */
-    int block_threads;  /* threads per block: 0 = default (128); 64, 128 or 256 */
+    int block_threads;  /* threads per block: 0 = default (128; 256 for RADM2_SCHED_COOP);
+                           32, 64, 128 or 256 (the built variants) */
     int blocks_per_sm;  /* persistent grid blocks per SM: 0 = default */
     int float_coeffs;   /* 1 (default): M/E rounded through float as mgpu.cu:3300-3304 */
     int placement;      /* working-set placement: RADM2_PLACE_* (default GLOBAL) */
@@ -322,6 +328,14 @@ int radm2_seed_cells(radm2_ctx *ctx, radm2_mlp *mlp, double dt, int set_h0, int 
  * state on the device first, inside the same CUDA graph for radm2_run_split.
  * set_order as for radm2_seed_cells. */
 int radm2_attach_mlp(radm2_ctx *ctx, radm2_mlp *mlp, int set_order);
+
+/* Self-test of the cooperative kernel's bounded waits (a context with schedule
+ * RADM2_SCHED_COOP and cells set): one integration in which a warp of every block waits on
+ * a flag that nothing sets, with a short limit (~1 ms).  The wait must run out, the blocks
+ * must return and the integration must report RADM2_E_CUDA.  RADM2_OK when it did,
+ * RADM2_E_STATE if not.  The cells' states are not changed; the context stays usable.  No
+ * counterpart in the reference. */
+int radm2_coop_selftest_wait_limit(radm2_ctx *ctx);
 
 /* Host-only consistency check of the library's kernel layouts (every thread's
  * working-set offsets inside its allocation, for every built variant). */

@@ -252,6 +252,10 @@ int key_of(const radm2_ctx *c, int bs)
 
 cudaError_t variant_info(radm2_ctx *c, int bs, SolverInfo *info)
 {
+    if (c->o.schedule == RADM2_SCHED_COOP) {
+        if (c->o.parity) return bs == 256 ? solver_info_coopx_g8(info) : cudaErrorInvalidValue;
+        return bs == 128 ? solver_info_coop_g4(info) : bs == 256 ? solver_info_coop_g8(info) : cudaErrorInvalidValue;
+    }
     const bool fp32 = c->o.precision == RADM2_PREC_FP32LU;
     const bool pers = c->o.schedule == RADM2_SCHED_PERSISTENT;
     const int k = key_of(c, bs);
@@ -264,6 +268,7 @@ cudaError_t variant_info(radm2_ctx *c, int bs, SolverInfo *info)
 
 int default_block_threads(const radm2_opts &o)
 {
+    if (o.schedule == RADM2_SCHED_COOP) return 256;
     if (o.placement == RADM2_PLACE_GLOBAL) return 128;
     if (o.placement == RADM2_PLACE_LU_SMEM && o.precision == RADM2_PREC_FP32LU) return 64;
     return 32;
@@ -280,7 +285,11 @@ int launch_geometry(radm2_ctx *c, int *bs_out, int *grid_out, size_t *scratch_ou
         return RADM2_E_ARG;
     }
     int grid;
-    if (c->o.schedule == RADM2_SCHED_PERSISTENT) {
+    if (c->o.schedule == RADM2_SCHED_COOP) {  // 32 cells per block, one block per SM
+        grid = c->nsm * info.blocks_per_sm;
+        const int need = (c->ncell + 31) / 32;
+        if (grid > need) grid = need;
+    } else if (c->o.schedule == RADM2_SCHED_PERSISTENT) {
         int bpsm = c->o.blocks_per_sm > 0 ? c->o.blocks_per_sm : info.blocks_per_sm;
         if (bpsm > info.blocks_per_sm) bpsm = info.blocks_per_sm;
         grid = c->nsm * bpsm;
@@ -293,6 +302,8 @@ int launch_geometry(radm2_ctx *c, int *bs_out, int *grid_out, size_t *scratch_ou
     *bs_out = bs;
     *grid_out = grid;
     *scratch_out = (size_t)grid * bs * info.global_words * sizeof(double);
+    if (c->o.schedule == RADM2_SCHED_COOP)  // per block: the rate constants of its 32 cells
+        *scratch_out = (size_t)grid * NREACT * 32 * sizeof(double);
     return RADM2_OK;
 }
 
@@ -329,6 +340,7 @@ SolveArgs make_args(radm2_ctx *c, const SolveParams &p, int *queue)
     a.hexit = c->hexit;
     a.texit = c->texit;
     a.refine = c->o.refine_sweeps;
+    a.coop_selftest = c->coop_selftest;
     return a;
 }
 
@@ -337,6 +349,10 @@ cudaError_t launch_solver(radm2_ctx *c, const SolveArgs &a, int bs, int grid)
     const bool fp32 = c->o.precision == RADM2_PREC_FP32LU;
     const bool pers = c->o.schedule == RADM2_SCHED_PERSISTENT;
     const int k = key_of(c, bs);
+    if (c->o.schedule == RADM2_SCHED_COOP) {
+        if (c->o.parity) return launch_solver_coopx_g8(a, grid, c->st);
+        return bs == 128 ? launch_solver_coop_g4(a, grid, c->st) : launch_solver_coop_g8(a, grid, c->st);
+    }
     if (c->o.parity)  // reference arithmetic: divisions kept, no multiply-add contraction
         return pers ? launch_solver_fp64x_persistent(a, k, grid, c->st) : launch_solver_fp64x_static(a, k, grid, c->st);
     if (fp32 && c->o.refine_sweeps == 0)  // the variants without the refinement code
@@ -427,6 +443,7 @@ int finish(radm2_ctx *c, int nres, int autonomous, double *RPAR, int *IPAR, int 
     c->stats.n_rejected = nrej;
     c->stats.n_failed = nfail;
     c->stats.worst_status = worst;
+    if (worst == RADM2_E_CUDA) c->err = "solver: a bounded wait between cooperating warps ran out";
     c->stats.max_steps_cell = max_att;
     c->stats.texit_min = RPAR[10];
     c->stats.hexit_min = hmin;
@@ -468,7 +485,11 @@ int radm2_create(radm2_ctx **out, const radm2_opts *opts)
     else
         radm2_opts_default(&o);
     if (o.precision != RADM2_PREC_FP64 && o.precision != RADM2_PREC_FP32LU) return RADM2_E_ARG;
-    if (o.schedule != RADM2_SCHED_STATIC && o.schedule != RADM2_SCHED_PERSISTENT) return RADM2_E_ARG;
+    if (o.schedule != RADM2_SCHED_STATIC && o.schedule != RADM2_SCHED_PERSISTENT && o.schedule != RADM2_SCHED_COOP)
+        return RADM2_E_ARG;
+    if (o.schedule == RADM2_SCHED_COOP &&
+        (o.precision != RADM2_PREC_FP64 || o.placement != RADM2_PLACE_GLOBAL || o.min_blocks > 1))
+        return RADM2_E_ARG;
     if (o.refine_sweeps < 0 || o.refine_sweeps > 2) return RADM2_E_ARG;
     if (o.placement != RADM2_PLACE_GLOBAL && o.placement != RADM2_PLACE_LU_SMEM && o.placement != RADM2_PLACE_ALL_SMEM)
         return RADM2_E_ARG;
@@ -789,7 +810,8 @@ int radm2_rosenbrock_host(radm2_ctx *c, int ncell, double *VAR, const double *FI
         a.hexit += lo;
         a.texit += lo;
         int kg = grid;
-        if (c->o.schedule == RADM2_SCHED_PERSISTENT) kg = std::min(grid, (m + bs - 1) / bs);
+        if (c->o.schedule == RADM2_SCHED_COOP) kg = std::min(grid, (m + 31) / 32);
+        else if (c->o.schedule == RADM2_SCHED_PERSISTENT) kg = std::min(grid, (m + bs - 1) / bs);
         else kg = (m + bs - 1) / bs;
         CK(launch_solver(c, a, bs, std::max(kg, 1)));
         CK(launch_reduce(m, c->status + lo, c->nacc + lo, c->nrej + lo, c->texit + lo, c->hexit + lo, c->partials,
@@ -1081,6 +1103,10 @@ int radm2_autotune(radm2_ctx *c, double dt, const double *AbsTol, const double *
         int sched, bs, place, minb;
     };
     std::vector<Cand> cands;
+    if (c->o.precision == RADM2_PREC_FP64) {  // cooperative blocks: 4 or 8 warps per 32 cells
+        if (!c->o.parity) cands.push_back({RADM2_SCHED_COOP, 128, RADM2_PLACE_GLOBAL, 1});
+        cands.push_back({RADM2_SCHED_COOP, 256, RADM2_PLACE_GLOBAL, 1});
+    }
     for (int sched = RADM2_SCHED_STATIC; sched <= RADM2_SCHED_PERSISTENT; sched++) {
 #define RADM2_TUNE_CAND(BS_, PL_, MB_) cands.push_back({sched, BS_, PL_, MB_});
         if (c->o.parity) {
@@ -1227,6 +1253,31 @@ size_t radm2_device_bytes(const radm2_ctx *c)
 {
     if (!c) return 0;
     return c->bytes + c->scratch_bytes + c->stage_bytes;
+}
+
+int radm2_coop_selftest_wait_limit(radm2_ctx *c)
+{
+    if (!valid_ctx(c)) return RADM2_E_ARG;
+    if (!c->var) return RADM2_E_STATE;
+    if (c->o.schedule != RADM2_SCHED_COOP) return RADM2_E_ARG;
+    double atol[NVAR], rtol[NVAR], rpar[20] = {0};
+    int ipar[20] = {0};
+    for (int i = 0; i < NVAR; i++) {
+        atol[i] = 1.0;
+        rtol[i] = 1e-3;
+    }
+    ipar[0] = 1;
+    ipar[3] = 2;
+    drop_graph(c);
+    // cells the aborted blocks never take keep their status: start from a neutral 0
+    CK(cudaMemsetAsync(c->status, 0, sizeof(int) * c->ld, c->st));
+    c->coop_selftest = 1;
+    const int ierr = radm2_rosenbrock(c, 0.0, 600.0, atol, rtol, rpar, ipar);
+    c->coop_selftest = 0;
+    drop_graph(c);
+    if (ierr != RADM2_E_CUDA) return RADM2_E_STATE;
+    c->err.clear();
+    return RADM2_OK;
 }
 
 int radm2_selfcheck(void)

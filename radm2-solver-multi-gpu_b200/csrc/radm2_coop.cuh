@@ -1,0 +1,425 @@
+// The cooperative per-cell ROS-3 solver kernel: a cell's working set on chip.
+//
+// A thread block holds 32 cells, one per lane, and G warps ("roles").  Every warp runs
+// lane-per-cell SIMT code over the block's 32 cells, but each phase of a step attempt is
+// split between the G roles (the split is generated by mech/emit_coop.py):
+//   RHS                  each role sums the right-hand side of the species it owns
+//   Jacobian             each role forms its share of the 659 slots, G = -J + I/(h gamma)
+//   LU                   each role eliminates its rows (row-Doolittle, mgpu.cu:2746-2779);
+//                        a row that needs another role's pivot row waits on that row's flag
+//   solves               forward rows, a block barrier, backward rows, likewise with flags
+//   stage vectors        each role keeps Fcn0, K1, K2, K3 of its own species in registers
+//   error norm           each role writes the terms of its species; every role then sums
+//                        all 59 in species order (the sequential sum of mgpu.cu:3223-3238),
+//                        so every role takes the same step-control decision
+// So one cell is served by G lanes (one in each warp), and its LU (5.3 KB), state and
+// stage right-hand side live in shared memory: 32 cells x 777 words = 199 KB per block,
+// one block per SM.  The rate constants of the block's cells are copied once per cell
+// into a small per-block slot array in global memory, [156][32] per block (40 KB, L1/L2
+// resident), so that every read is a fixed offset from the lane's base address; per step
+// attempt nothing else of a cell touches global memory.
+//
+// Cells come from the same work queue as the persistent schedule: lanes whose cell
+// finished take the next queue entries (warp-aggregated atomic in role 0) between
+// attempts, so lanes never wait for the slowest cell of the block.
+//
+// Waits on another role's row flag are bounded (COOP_WAIT_CYCLES of the SM clock, about
+// one second); a wait that runs out marks the block's cells with status RADM2_E_CUDA and
+// the block returns, so a fault in the schedule ends the launch with an error instead of
+// hanging the GPU.
+//
+// This header is included by one instantiation file per kernel, which defines
+//   RADM2_COOP_G       roles (warps) per block: 4 or 8
+//   RADM2_COOP_RECIP   1 = reciprocal pivots (the fast form), 0 = the reference's divisions
+//                      (that file is compiled without multiply-add contraction)
+//   RADM2_COOP_KERNEL  the kernel's name
+#pragma once
+
+#include "radm2_device.cuh"
+
+#if RADM2_COOP_G == 4
+#include "gen/radm2_coop_g4.h"
+#define RADM2_COOP_NS RADM2_COOP_G4_NS
+#define RADM2_COOP_OWN_INC "gen/radm2_coop_g4_own.inc"
+#define RADM2_COOP_FUN_INC "gen/radm2_coop_g4_fun.inc"
+#define RADM2_COOP_JAC_INC "gen/radm2_coop_g4_jac.inc"
+#define RADM2_COOP_FWD_INC "gen/radm2_coop_g4_fwd.inc"
+#if RADM2_COOP_RECIP
+#define RADM2_COOP_LU_INC "gen/radm2_coop_g4_lu.inc"
+#define RADM2_COOP_BWD_INC "gen/radm2_coop_g4_bwd.inc"
+#else
+#define RADM2_COOP_LU_INC "gen/radm2_coop_g4_lu_div.inc"
+#define RADM2_COOP_BWD_INC "gen/radm2_coop_g4_bwd_div.inc"
+#endif
+#elif RADM2_COOP_G == 8
+#include "gen/radm2_coop_g8.h"
+#define RADM2_COOP_NS RADM2_COOP_G8_NS
+#define RADM2_COOP_OWN_INC "gen/radm2_coop_g8_own.inc"
+#define RADM2_COOP_FUN_INC "gen/radm2_coop_g8_fun.inc"
+#define RADM2_COOP_JAC_INC "gen/radm2_coop_g8_jac.inc"
+#define RADM2_COOP_FWD_INC "gen/radm2_coop_g8_fwd.inc"
+#if RADM2_COOP_RECIP
+#define RADM2_COOP_LU_INC "gen/radm2_coop_g8_lu.inc"
+#define RADM2_COOP_BWD_INC "gen/radm2_coop_g8_bwd.inc"
+#else
+#define RADM2_COOP_LU_INC "gen/radm2_coop_g8_lu_div.inc"
+#define RADM2_COOP_BWD_INC "gen/radm2_coop_g8_bwd_div.inc"
+#endif
+#else
+#error "RADM2_COOP_G must be 4 or 8"
+#endif
+
+namespace radm2 {
+
+// Shared-memory layout of a block, in doubles: word w of lane l at w * 32 + l.
+constexpr int COOP_LU = 0;                     // the 659 LU slots
+constexpr int COOP_Y = NJVS;                   // state Y
+constexpr int COOP_X = NJVS + NVAR;            // stage right-hand side / solution, error terms
+constexpr int COOP_DWORDS = NJVS + 2 * NVAR;   // 777
+// then ints
+constexpr int COOP_FLAG_LU = 0;                // [64] LU row flags
+constexpr int COOP_FLAG_SV = 64;               // [64] solve row flags
+constexpr int COOP_FLAG_NEVER = 127;           // a flag no row sets (wait-limit self-test)
+constexpr int COOP_CELL = 128;                 // [32] cell taken by each lane (-1: none)
+constexpr int COOP_SING = 160;                 // [32] zero pivot seen in this attempt
+constexpr int COOP_ERR = 192;                  // block error flag (a wait ran out)
+constexpr int COOP_IWORDS = 224;
+constexpr size_t COOP_SMEM_BYTES = (size_t)COOP_DWORDS * 32 * sizeof(double) + COOP_IWORDS * sizeof(int);
+static_assert(COOP_SMEM_BYTES <= 227 * 1024, "cooperative block does not fit shared memory");
+
+constexpr long long COOP_WAIT_CYCLES = 1ll << 31;  // ~1 s at 2 GHz
+constexpr int COOP_STATUS_WAIT_LIMIT = -101;        // RADM2_E_CUDA: a wait ran out
+constexpr long long COOP_SELFTEST_WAIT_CYCLES = 1ll << 20;
+
+// Publish a finished row: every lane's stores are ordered before the flag, which one lane
+// sets once the whole warp has stored.
+__device__ __forceinline__ void coop_signal(volatile int *flag, int seq)
+{
+    __threadfence_block();
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0) {
+        __threadfence_block();
+        *flag = seq;
+    }
+}
+
+// Wait until another role published the row (flag >= seq), at most `limit` SM cycles.
+// After one wait has run out, later waits of the thread return at once: the block only
+// runs on to its error exit at the end of the attempt.
+__device__ __forceinline__ void coop_wait(volatile int *flag, int seq, int *werr, long long limit)
+{
+    if (*werr) return;
+    if (*flag < seq) {
+        const long long t0 = clock64();
+        while (*flag < seq) {
+            if (clock64() - t0 > limit) {
+                *werr = 1;
+                break;
+            }
+        }
+    }
+    __threadfence_block();  // the row's loads stay after the flag
+}
+
+__global__ void __launch_bounds__(32 * RADM2_COOP_G, 1) RADM2_COOP_KERNEL(const SolveArgs a)
+{
+    constexpr int NS = RADM2_COOP_NS;
+    extern __shared__ double smem[];
+    double *const lu = smem + COOP_LU * 32;
+    double *const ys = smem + COOP_Y * 32;
+    double *const xs = smem + COOP_X * 32;
+    int *const ism = reinterpret_cast<int *>(smem + COOP_DWORDS * 32);
+    volatile int *const vflag = ism;
+    const int lane = threadIdx.x & 31;
+    const int role = threadIdx.x >> 5;
+    const SolveParams &P = a.p;
+    const int ld = a.ld;
+    const int dir = P.direction;
+
+    for (int i = threadIdx.x; i < COOP_IWORDS; i += blockDim.x) ism[i] = (i >= COOP_CELL && i < COOP_CELL + 32) ? -1 : 0;
+    __syncthreads();
+
+    // ---- lane state, the same in every role
+    bool have = false;   // the lane holds a cell
+    bool fetch = true;   // the lane's cell finished (or none yet): results out, next cell in
+    bool outer = false;  // the next attempt starts a step: Fcn0 first
+    int cidx = 0;
+    double T = 0.0, H = 0.0, fix0 = 0.0, fix1 = 0.0, hfirst = 0.0;
+    int rlast = 0, rmore = 0, nacc = 0, nrej = 0, nstp = 0, status = 1;
+    double *const rcs = a.scratch + (size_t)blockIdx.x * NREACT * 32 + lane;  // [156][32] per block
+    // ---- the role's own species: stage vectors in registers
+    double f0[NS], k1[NS], k2[NS], k3[NS];
+#pragma unroll
+    for (int k = 0; k < NS; k++) f0[k] = k1[k] = k2[k] = k3[k] = 0.0;
+    int lu_seq = 0, sv_seq = 0, werr = 0;
+
+#define COOP_ROLE role
+#define RC(r) rcs[(r) * 32]
+#define FIX(k) ((k) == 0 ? fix0 : fix1)
+#define SW(base, w) (base)[(w) * 32 + lane]
+#define COOP_FENCE asm volatile("" ::: "memory")
+
+    for (;;) {
+        // ================================================================ cells out / in
+        if (fetch && have) {
+            double *v = a.var + cidx;
+#define OWN(k, s) v[(size_t)(s) * ld] = SW(ys, s);
+#include RADM2_COOP_OWN_INC
+#undef OWN
+            if (role == 0) {
+                a.status[cidx] = status;
+                a.nacc[cidx] = nacc;
+                a.nrej[cidx] = nrej;
+                a.hfirst[cidx] = hfirst;
+                a.hexit[cidx] = H;
+                a.texit[cidx] = T;
+            }
+            have = false;
+        }
+        if (role == 0) {
+            const unsigned m = __ballot_sync(0xffffffffu, fetch);
+            if (m) {
+                const int leader = __ffs(m) - 1;
+                int base = 0;
+                if (lane == leader) base = atomicAdd(a.queue, __popc(m));
+                base = __shfl_sync(0xffffffffu, base, leader);
+                if (fetch) {
+                    const int c = base + __popc(m & ((1u << lane) - 1));
+                    ism[COOP_CELL + lane] = c < a.ncell ? c : -1;
+                }
+            }
+        }
+        __syncthreads();
+        if (fetch) {
+            const int c = ism[COOP_CELL + lane];
+            fetch = false;
+            if (c >= 0) {
+                have = true;
+                cidx = a.order ? a.order[c] : c;
+                const double *v = a.var + cidx;
+                const double *rc = a.rconst + cidx;
+                for (int r = role; r < NREACT; r += RADM2_COOP_G) rcs[r * 32] = rc[(size_t)r * ld];
+#define OWN(k, s) SW(ys, s) = v[(size_t)(s) * ld];
+#include RADM2_COOP_OWN_INC
+#undef OWN
+                fix0 = a.fix[cidx];
+                fix1 = a.fix[(size_t)ld + cidx];
+                T = P.Tstart;
+                double hs = P.Hstart;
+                if (a.h0) {
+                    const double h = a.h0[cidx];
+                    if (h > 0.0 && h <= P.Hmax) hs = h;  // non-finite or out of range: default
+                }
+                H = mind(hs, P.Hmax);  // mgpu.cu:3475-3477
+                if (absd(H) <= 10.0 * P.Roundoff) H = DELTA_MIN;
+                rlast = rmore = nacc = nrej = nstp = 0;
+                status = 1;
+                hfirst = 0.0;
+                // time-loop mask (mgpu.cu:1608-1613) and the clamp to the remaining interval
+                const bool more = (dir > 0 && (T - P.Tend) + P.Roundoff <= 0.0) ||
+                                  (dir < 0 && (P.Tend - T) + P.Roundoff <= 0.0);
+                if (more) {
+                    H = mind(H, absd(P.Tend - T));
+                    outer = true;
+                } else {
+                    fetch = true;  // nothing to integrate: out again at the next turn
+                }
+            }
+        }
+        if (!__syncthreads_or(have)) break;  // also orders the state loads before the RHS
+
+        // ================================================================ Fcn0 = F(Y)
+        if (__syncthreads_or(outer)) {
+            double fo[NS];
+#define V(i) SW(ys, i)
+#define FUN_OUT(k, e) fo[k] = (e)
+#include RADM2_COOP_FUN_INC
+#undef FUN_OUT
+#undef V
+#pragma unroll
+            for (int k = 0; k < NS; k++)
+                if (outer) f0[k] = fo[k];
+        }
+        outer = false;
+
+        // ================================================================ one attempt
+        bool active = have && !fetch;
+        if (active && nstp >= P.max_steps) {
+            status = -6;
+            fetch = true;
+            active = false;
+        }
+        if (active && ((T + 0.1 * H == T) || (H <= P.Roundoff))) {
+            status = -7;
+            fetch = true;
+            active = false;
+        }
+        const double ghinv = 1.0 / (dir * H * RADM2_ROS_GAMMA0);
+        // G = -J(Y) + ghinv I into the LU slots; the stage-1 right-hand side Fcn0
+        {
+#define V(i) SW(ys, i)
+#define JAC_OUT(s, e) SW(lu, s) = -(e)
+#define JAC_OUT_DIAG(s, e) SW(lu, s) = (-(e)) + ghinv
+#define JAC_OUT_ZERO(s, d) SW(lu, s) = (d) ? ((-0.0) + ghinv) : (-0.0)
+#include RADM2_COOP_JAC_INC
+#undef JAC_OUT
+#undef JAC_OUT_DIAG
+#undef JAC_OUT_ZERO
+#undef V
+        }
+#define OWN(k, s) SW(xs, s) = f0[k];
+#include RADM2_COOP_OWN_INC
+#undef OWN
+        if (role == 0) ism[COOP_SING + lane] = 0;
+        __syncthreads();
+
+        // LU, rows split between the roles
+        lu_seq++;
+        if (a.coop_selftest && role == 1)  // a flag nothing sets: the bounded wait runs out
+            coop_wait(vflag + COOP_FLAG_NEVER, lu_seq, &werr, COOP_SELFTEST_WAIT_CYCLES);
+        {
+#define G(s) SW(lu, s)
+#define LU_T double
+#define LU_PIVOT_CHECK(k, v) \
+    if ((v) == 0.0) ism[COOP_SING + lane] = 1
+#define LU_WAIT(j) coop_wait(vflag + COOP_FLAG_LU + (j), lu_seq, &werr, COOP_WAIT_CYCLES)
+#define LU_DONE(i) coop_signal(vflag + COOP_FLAG_LU + (i), lu_seq)
+#include RADM2_COOP_LU_INC
+#undef LU_WAIT
+#undef LU_DONE
+#undef LU_PIVOT_CHECK
+#undef LU_T
+#undef G
+        }
+        __syncthreads();
+        if (active && ism[COOP_SING + lane]) {
+            status = -8;
+            fetch = true;
+            active = false;
+        }
+        const double hc21 = RADM2_ROS_C0 / (dir * H);
+        const double hc31 = RADM2_ROS_C1 / (dir * H);
+        const double hc32 = RADM2_ROS_C2 / (dir * H);
+
+        // ---- the three stages, one solve each: stage 1 K1 = G^-1 Fcn0; stage 2 the RHS
+        // F(Y + A21 K1) + C21/h K1; stage 3 reuses that F (NewF = 0) with C31/h K1 + C32/h K2
+#pragma unroll 1
+        for (int stage = 0; stage < 3; stage++) {
+            if (stage == 1) {
+#define OWN(k, s)                                     \
+    {                                                 \
+        k1[k] = SW(xs, s);                            \
+        SW(xs, s) = SW(ys, s) + RADM2_ROS_A0 * k1[k]; \
+    }
+#include RADM2_COOP_OWN_INC
+#undef OWN
+                __syncthreads();
+                double fo[NS];
+#define V(i) SW(xs, i)
+#define FUN_OUT(k, e) fo[k] = (e)
+#include RADM2_COOP_FUN_INC
+#undef FUN_OUT
+#undef V
+                __syncthreads();  // every role has read Y + A21 K1
+#define OWN(k, s)                          \
+    {                                      \
+        SW(xs, s) = fo[k] + k1[k] * hc21;  \
+        k3[k] = fo[k] + k1[k] * hc31;      \
+    }
+#include RADM2_COOP_OWN_INC
+#undef OWN
+                __syncthreads();
+            } else if (stage == 2) {
+#define OWN(k, s)                          \
+    {                                      \
+        k2[k] = SW(xs, s);                 \
+        SW(xs, s) = k3[k] + k2[k] * hc32;  \
+    }
+#include RADM2_COOP_OWN_INC
+#undef OWN
+                __syncthreads();
+            }
+            // forward rows (flags), barrier, backward rows (flags), barrier
+#define G(s) SW(lu, s)
+#define X(i) SW(xs, i)
+#define SOLVE_WAIT(j) coop_wait(vflag + COOP_FLAG_SV + (j), sv_seq, &werr, COOP_WAIT_CYCLES)
+#define SOLVE_DONE(i) coop_signal(vflag + COOP_FLAG_SV + (i), sv_seq)
+            sv_seq++;
+#include RADM2_COOP_FWD_INC
+            __syncthreads();
+            sv_seq++;
+#include RADM2_COOP_BWD_INC
+            __syncthreads();
+#undef SOLVE_WAIT
+#undef SOLVE_DONE
+#undef X
+#undef G
+        }
+
+        // ================================================================ error norm, step control
+        // (mgpu.cu:3223-3260): each role its species' terms, then every role the ordered sum
+        double yn[NS];
+#define OWN(k, s)                                                                   \
+    {                                                                               \
+        k3[k] = SW(xs, s);                                                          \
+        const double y = SW(ys, s);                                                 \
+        yn[k] = P.M[0] * k1[k] + P.M[1] * k2[k] + P.M[2] * k3[k] + y;              \
+        const double yerr = P.E[0] * k1[k] + P.E[1] * k2[k] + P.E[2] * k3[k];      \
+        const double ymax = maxd(absd(y), absd(yn[k]));                             \
+        const double scale = P.AbsTol[s] + P.RelTol[s] * ymax;                      \
+        SW(xs, s) = (yerr * yerr) / (scale * scale);                                \
+    }
+#include RADM2_COOP_OWN_INC
+#undef OWN
+        if (werr) ism[COOP_ERR] = 1;
+        __syncthreads();
+        if (ism[COOP_ERR]) {
+            // a bounded wait ran out: this block's cells end with an error status
+            if (role == 0 && have) a.status[cidx] = COOP_STATUS_WAIT_LIMIT;
+            break;
+        }
+        double err = 0.0;
+#pragma unroll
+        for (int i = 0; i < NVAR; i++) err += SW(xs, i);
+        err = sqrt(err / (double)NVAR);
+        const double fac = mind(P.FacMax, maxd(P.FacMin, P.FacSafe / pow(err, 1.0 / RADM2_ROS_ELO)));
+        double hnew = H * fac;
+        if (err != err) hnew = H * P.FacRej;  // non-finite norm: shrink hard and retry
+        if (active) {
+            nstp++;
+            if ((err <= 1.0) || (H <= P.Hmin)) {
+#define OWN(k, s) SW(ys, s) = yn[k];
+#include RADM2_COOP_OWN_INC
+#undef OWN
+                T += dir * H;
+                if (rlast) hnew = mind(hnew, H);
+                rlast = 0;
+                rmore = 0;
+                if (nacc == 0) hfirst = H;
+                nacc++;
+                H = hnew;
+                const bool more = (dir > 0 && (T - P.Tend) + P.Roundoff <= 0.0) ||
+                                  (dir < 0 && (P.Tend - T) + P.Roundoff <= 0.0);
+                if (more) {
+                    H = mind(H, absd(P.Tend - T));
+                    outer = true;
+                } else {
+                    fetch = true;
+                }
+            } else {
+                if (rmore) hnew = H * P.FacRej;
+                rmore = rlast;
+                rlast = 1;
+                nrej++;
+                H = hnew;
+            }
+        }
+    }
+#undef COOP_FENCE
+#undef SW
+#undef FIX
+#undef RC
+#undef COOP_ROLE
+}
+
+}  // namespace radm2

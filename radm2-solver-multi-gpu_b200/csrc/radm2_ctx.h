@@ -54,6 +54,7 @@ struct radm2_ctx {
     bool use_h0 = true, use_order = true;  // whether the solver reads h0 / order when set
     radm2_mlp *mlp = nullptr;               // attached network: seeds every integration
     int mlp_order = 0;  // 0 none, 1 cells by predicted cost, 2 chunks of 32 cells by cost
+    int coop_selftest = 0;  // next integrations: the cooperative kernel's wait-limit self-test
 };
 
 namespace radm2 {

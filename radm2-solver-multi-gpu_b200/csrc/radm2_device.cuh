@@ -88,6 +88,7 @@ struct SolveArgs {
     int *nacc, *nrej;
     double *hfirst, *hexit, *texit;
     int refine;              // FP32 LU: FP64 refinement sweeps per stage solve
+    int coop_selftest;       // cooperative kernel: one role waits on a flag nothing sets
 };
 
 // Per-thread scratch, in double words.  Laid out word-major inside each block

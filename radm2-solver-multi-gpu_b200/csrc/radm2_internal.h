@@ -56,6 +56,12 @@ cudaError_t launch_reduce(int n, const int *status, const int *nacc, const int *
 // Reference-arithmetic FP64 solver (radm2_opts.parity): global placement only.
 #define RADM2_VARIANTS_FP64X(X) X(32, 0, 1) X(64, 0, 1) X(128, 0, 1) X(256, 0, 1)
 
+// Cooperative kernels (radm2_coop.cuh): 32 cells per block, G roles (warps) per block,
+// one block per SM; the "x" kernel keeps the reference's arithmetic.
+cudaError_t launch_solver_coop_g4(const SolveArgs &a, int grid, cudaStream_t st);
+cudaError_t launch_solver_coop_g8(const SolveArgs &a, int grid, cudaStream_t st);
+cudaError_t launch_solver_coopx_g8(const SolveArgs &a, int grid, cudaStream_t st);
+
 // Static properties of one solver variant on the current device.
 struct SolverInfo {
     int regs;           // registers per thread
@@ -87,6 +93,9 @@ cudaError_t solver_info_fp32d_static(int key, SolverInfo *out);
 cudaError_t solver_info_fp32d_persistent(int key, SolverInfo *out);
 cudaError_t solver_info_fp64x_static(int key, SolverInfo *out);
 cudaError_t solver_info_fp64x_persistent(int key, SolverInfo *out);
+cudaError_t solver_info_coop_g4(SolverInfo *out);
+cudaError_t solver_info_coop_g8(SolverInfo *out);
+cudaError_t solver_info_coopx_g8(SolverInfo *out);
 // Host-side bounds check of every built variant's working-set layout (0 = all in bounds).
 int solver_layout_check_fp64_static();
 int solver_layout_check_fp64_persistent();

@@ -1,0 +1,37 @@
+// Instantiation of the cooperative solver kernel: 8 roles per block of 32 cells in reference arithmetic (divisions kept; built without multiply-add contraction).
+#define RADM2_COOP_G 8
+#define RADM2_COOP_RECIP 0
+#define RADM2_COOP_KERNEL k_rosenbrock_coopx_g8
+#include "radm2_internal.h"
+#include "radm2_coop.cuh"
+
+namespace radm2 {
+
+cudaError_t launch_solver_coopx_g8(const SolveArgs &a, int grid, cudaStream_t st)
+{
+    cudaError_t e = cudaFuncSetAttribute(k_rosenbrock_coopx_g8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)COOP_SMEM_BYTES);
+    if (e != cudaSuccess) return e;
+    (void)cudaGetLastError();  // a stale error from another library is not this launch's
+    k_rosenbrock_coopx_g8<<<grid, 32 * RADM2_COOP_G, COOP_SMEM_BYTES, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t solver_info_coopx_g8(SolverInfo *out)
+{
+    cudaFuncAttributes at{};
+    cudaError_t e = cudaFuncGetAttributes(&at, k_rosenbrock_coopx_g8);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_rosenbrock_coopx_g8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)COOP_SMEM_BYTES);
+    if (e != cudaSuccess) return e;
+    int blocks = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_rosenbrock_coopx_g8, 32 * RADM2_COOP_G, COOP_SMEM_BYTES);
+    if (e != cudaSuccess) return e;
+    out->regs = at.numRegs;
+    out->local_bytes = (int)at.localSizeBytes;
+    out->blocks_per_sm = blocks;
+    out->global_words = 0;
+    out->smem_bytes = (int)COOP_SMEM_BYTES;
+    return cudaSuccess;
+}
+
+}  // namespace radm2

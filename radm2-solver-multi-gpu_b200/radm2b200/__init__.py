@@ -5,5 +5,5 @@
     seeding  step traces, training and use of the step-seeding network
 """
 from . import inputs  # noqa: F401
-from .lib import (NFIX, NJVS, NPH, NREACT, NVAR, PREC_FP32LU, PREC_FP64, SCHED_PERSISTENT,  # noqa: F401
+from .lib import (NFIX, NJVS, NPH, NREACT, NVAR, PREC_FP32LU, PREC_FP64, SCHED_COOP, SCHED_PERSISTENT,  # noqa: F401
                   SCHED_STATIC, Mlp, RadmError, Solver, add_step_counters, default_params, fma_peak, load)

@@ -16,7 +16,7 @@ import numpy as np
 NVAR, NFIX, NREACT, NPH, NJVS = 59, 2, 156, 28, 659
 PREC_FP64, PREC_FP32LU = 0, 1
 PLACE_GLOBAL, PLACE_LU_SMEM, PLACE_ALL_SMEM = 0, 1, 3
-SCHED_STATIC, SCHED_PERSISTENT = 0, 1
+SCHED_STATIC, SCHED_PERSISTENT, SCHED_COOP = 0, 1, 2
 RADM2_OK, RADM2_E_ARG, RADM2_E_CUDA, RADM2_E_NOMEM, RADM2_E_STATE, RADM2_E_NODEV, RADM2_E_TOOBIG = \
     0, -100, -101, -102, -103, -104, -105
 
@@ -124,6 +124,7 @@ SIGNATURES = {
                                                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double,
                                                  ctypes.c_double, _D, _D, _D, _I, ctypes.c_void_p, ctypes.c_void_p]),
     "radm2_selfcheck": (ctypes.c_int, []),
+    "radm2_coop_selftest_wait_limit": (ctypes.c_int, [ctypes.c_void_p]),
     "radm2_version": (ctypes.c_char_p, []),
 }
 
@@ -344,6 +345,11 @@ class Solver:
 
     def device_bytes(self):
         return int(self.lib.radm2_device_bytes(self.h))
+
+    def coop_selftest_wait_limit(self):
+        """Cooperative kernel: one integration in which a warp of every block waits on a
+        flag nothing sets; the bounded wait must run out and be reported (raises if not)."""
+        self._check(self.lib.radm2_coop_selftest_wait_limit(self.h))
 
     # ---- learned seeding
     def features(self, dt):
