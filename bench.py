@@ -345,10 +345,13 @@ def main():
             t0 = time.perf_counter()
             table = solver.autotune(dt, atol, arm_rtol)
             o = solver.opts()
-            tuned = {"chosen": {k: o[k] for k in ("schedule", "block_threads", "placement", "min_blocks")},
+            tuned = {"chosen": {k: o[k] for k in ("schedule", "block_threads", "placement", "min_blocks",
+                                                  "cells_per_thread")},
                      "seconds": time.perf_counter() - t0, "sample_cells": min(ncell, 262144),
+                     "candidates_columns": ["schedule", "block_threads", "placement", "min_blocks",
+                                            "cells_per_thread", "ms"],
                      "candidates": [[t["schedule"], t["block_threads"], t["placement"], t["min_blocks"],
-                                     round(t["ms"], 2)] for t in table]}
+                                     t["cells_per_thread"], round(t["ms"], 2)] for t in table]}
         if attach:
             solver.attach_mlp(net)
         y0 = torch.empty((59, ld), dtype=torch.float64, device="cuda")
@@ -436,7 +439,7 @@ def main():
         return radm2b200.Solver(precision=prec, refine_sweeps=refine, device=local,
                                 schedule=tuned_opts["schedule"], block_threads=tuned_opts["block_threads"],
                                 placement=tuned_opts["placement"], min_blocks=tuned_opts["min_blocks"],
-                                parity=tuned_opts["parity"])
+                                parity=tuned_opts["parity"], cells_per_thread=tuned_opts["cells_per_thread"])
 
     # ---- plain FP64 GPU solver on the same K splits (static cell-per-thread, default Hstart)
     plain = None
@@ -611,8 +614,8 @@ def main():
         line["autotune"] = main_arm["tuned"]
         ch = main_arm["tuned"]["chosen"]
         line["config"]["schedule"] = SCHED_NAMES[ch["schedule"]]
-        line["config"]["launch"] = "%d threads/block, placement %d, min blocks %d (autotuned)" % (
-            ch["block_threads"], ch["placement"], ch["min_blocks"])
+        line["config"]["launch"] = "%d threads/block, placement %d, min blocks %d, %d cell(s) per thread (autotuned)" % (
+            ch["block_threads"], ch["placement"], ch["min_blocks"], ch["cells_per_thread"])
     if train is not None:
         line["training"] = train
     if plain is not None:

@@ -71,6 +71,9 @@ typedef struct radm2_opts {
                            every operation rounds as the reference's C expressions do
                            (FP64 only; global placement; default 0 = the fast solver, which
                            multiplies by reciprocal pivots and contracts multiply-adds) */
+    int cells_per_thread; /* 1 (default) or 2: with 2, every thread of the thread-per-cell
+                           solver integrates two cells side by side (FP64, global placement,
+                           64 or 128 threads per block, static or persistent schedule) */
 } radm2_opts;
 
 /* Placement of each thread's working set (rate constants + state, and the LU). */
@@ -257,7 +260,8 @@ int radm2_get_opts(const radm2_ctx *ctx, radm2_opts *out);  /* options in force 
 /* Autotuner (no counterpart in the reference, which has one fixed launch shape).  Times
  * every built solver variant of the context's precision -- static and persistent
  * schedules x block size x placement of the working set (global scratch / shared memory)
- * x register cap -- on a strided sample of the context's current cells (sample_cells;
+ * x register cap, two cells per thread, and the cooperative blocks of 4 or 8 warps per 32
+ * cells (FP64) -- on a strided sample of the context's current cells (sample_cells;
  * 0 = 262,144) for one split of length dt with the given tolerances and parameters, and
  * keeps the fastest in the context's options (radm2_get_opts reads them).  Candidates
  * within 2x of the best first-pass time are timed a second time and keep the faster of
@@ -268,6 +272,7 @@ typedef struct radm2_tune_entry {
     int schedule, block_threads, placement, min_blocks; /* the candidate */
     double ms;                                          /* solver-kernel time, -1 = did not run */
     long long attempts;                                 /* step attempts of the sample split */
+    int cells_per_thread;                               /* 1 or 2 */
 } radm2_tune_entry;
 int radm2_autotune(radm2_ctx *ctx, double dt, const double *AbsTol, const double *RelTol, const double *RPAR,
                    const int *IPAR, int sample_cells, radm2_tune_entry *table, int table_len, int *n_entries);

@@ -252,6 +252,7 @@ int key_of(const radm2_ctx *c, int bs)
 
 cudaError_t variant_info(radm2_ctx *c, int bs, SolverInfo *info)
 {
+    if (c->o.cells_per_thread == 2) return solver_info_cpt2(bs, c->o.schedule, info);
     if (c->o.schedule == RADM2_SCHED_COOP) {
         if (c->o.parity) return bs == 256 ? solver_info_coopx_g8(info) : cudaErrorInvalidValue;
         return bs == 128 ? solver_info_coop_g4(info) : bs == 256 ? solver_info_coop_g8(info) : cudaErrorInvalidValue;
@@ -284,6 +285,7 @@ int launch_geometry(radm2_ctx *c, int *bs_out, int *grid_out, size_t *scratch_ou
         (void)cudaGetLastError();
         return RADM2_E_ARG;
     }
+    const int cpb = bs * (c->o.cells_per_thread == 2 ? 2 : 1);  // cells per block
     int grid;
     if (c->o.schedule == RADM2_SCHED_COOP) {  // 32 cells per block, one block per SM
         grid = c->nsm * info.blocks_per_sm;
@@ -293,10 +295,10 @@ int launch_geometry(radm2_ctx *c, int *bs_out, int *grid_out, size_t *scratch_ou
         int bpsm = c->o.blocks_per_sm > 0 ? c->o.blocks_per_sm : info.blocks_per_sm;
         if (bpsm > info.blocks_per_sm) bpsm = info.blocks_per_sm;
         grid = c->nsm * bpsm;
-        const int need = (c->ncell + bs - 1) / bs;
+        const int need = (c->ncell + cpb - 1) / cpb;
         if (grid > need) grid = need;
     } else {
-        grid = (c->ncell + bs - 1) / bs;
+        grid = (c->ncell + cpb - 1) / cpb;
     }
     if (grid < 1) grid = 1;
     *bs_out = bs;
@@ -349,6 +351,7 @@ cudaError_t launch_solver(radm2_ctx *c, const SolveArgs &a, int bs, int grid)
     const bool fp32 = c->o.precision == RADM2_PREC_FP32LU;
     const bool pers = c->o.schedule == RADM2_SCHED_PERSISTENT;
     const int k = key_of(c, bs);
+    if (c->o.cells_per_thread == 2) return launch_solver_cpt2(a, bs, c->o.schedule, grid, c->st);
     if (c->o.schedule == RADM2_SCHED_COOP) {
         if (c->o.parity) return launch_solver_coopx_g8(a, grid, c->st);
         return bs == 128 ? launch_solver_coop_g4(a, grid, c->st) : launch_solver_coop_g8(a, grid, c->st);
@@ -472,6 +475,7 @@ int radm2_opts_default(radm2_opts *o)
     o->placement = RADM2_PLACE_GLOBAL;
     o->min_blocks = 0;
     o->parity = 0;
+    o->cells_per_thread = 1;
     return RADM2_OK;
 }
 
@@ -494,6 +498,11 @@ int radm2_create(radm2_ctx **out, const radm2_opts *opts)
     if (o.placement != RADM2_PLACE_GLOBAL && o.placement != RADM2_PLACE_LU_SMEM && o.placement != RADM2_PLACE_ALL_SMEM)
         return RADM2_E_ARG;
     if (o.parity != 0 && o.parity != 1) return RADM2_E_ARG;
+    if (o.cells_per_thread == 0) o.cells_per_thread = 1;
+    if (o.cells_per_thread != 1 && o.cells_per_thread != 2) return RADM2_E_ARG;
+    if (o.cells_per_thread == 2 && (o.precision != RADM2_PREC_FP64 || o.placement != RADM2_PLACE_GLOBAL ||
+                                    o.min_blocks > 1 || o.parity || o.schedule == RADM2_SCHED_COOP))
+        return RADM2_E_ARG;
     if (o.parity && (o.precision != RADM2_PREC_FP64 || o.placement != RADM2_PLACE_GLOBAL)) return RADM2_E_ARG;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= o.device || o.device < 0) return RADM2_E_NODEV;
@@ -810,9 +819,10 @@ int radm2_rosenbrock_host(radm2_ctx *c, int ncell, double *VAR, const double *FI
         a.hexit += lo;
         a.texit += lo;
         int kg = grid;
+        const int cpb = bs * (c->o.cells_per_thread == 2 ? 2 : 1);
         if (c->o.schedule == RADM2_SCHED_COOP) kg = std::min(grid, (m + 31) / 32);
-        else if (c->o.schedule == RADM2_SCHED_PERSISTENT) kg = std::min(grid, (m + bs - 1) / bs);
-        else kg = (m + bs - 1) / bs;
+        else if (c->o.schedule == RADM2_SCHED_PERSISTENT) kg = std::min(grid, (m + cpb - 1) / cpb);
+        else kg = (m + cpb - 1) / cpb;
         CK(launch_solver(c, a, bs, std::max(kg, 1)));
         CK(launch_reduce(m, c->status + lo, c->nacc + lo, c->nrej + lo, c->texit + lo, c->hexit + lo, c->partials,
                          c->d_res + k, c->st));
@@ -877,7 +887,8 @@ int radm2_run_split(radm2_ctx *c, int nsplit, double dt, const double *AbsTol, c
         const uintptr_t extra[9] = {(uintptr_t)nsplit,
                                     (uintptr_t)bs,
                                     (uintptr_t)grid,
-                                    (uintptr_t)((c->o.parity * 4 + c->o.precision * 2 + c->o.schedule) * (1ull << 32) +
+                                    (uintptr_t)((c->o.cells_per_thread * 64 + c->o.parity * 16 + c->o.precision * 4 +
+                                                 c->o.schedule) * (1ull << 32) +
                                                 (unsigned)key_of(c, bs)),
                                     reinterpret_cast<uintptr_t>(c->mlp),
                                     (uintptr_t)mlp_generation(c->mlp),
@@ -1100,15 +1111,18 @@ int radm2_autotune(radm2_ctx *c, double dt, const double *AbsTol, const double *
     const int stride = c->ncell / n;
 
     struct Cand {
-        int sched, bs, place, minb;
+        int sched, bs, place, minb, cpt;
     };
     std::vector<Cand> cands;
     if (c->o.precision == RADM2_PREC_FP64) {  // cooperative blocks: 4 or 8 warps per 32 cells
-        if (!c->o.parity) cands.push_back({RADM2_SCHED_COOP, 128, RADM2_PLACE_GLOBAL, 1});
-        cands.push_back({RADM2_SCHED_COOP, 256, RADM2_PLACE_GLOBAL, 1});
+        if (!c->o.parity) cands.push_back({RADM2_SCHED_COOP, 128, RADM2_PLACE_GLOBAL, 1, 1});
+        cands.push_back({RADM2_SCHED_COOP, 256, RADM2_PLACE_GLOBAL, 1, 1});
+        if (!c->o.parity)  // two cells per thread
+            for (int sched = RADM2_SCHED_STATIC; sched <= RADM2_SCHED_PERSISTENT; sched++)
+                for (int bs : {64, 128}) cands.push_back({sched, bs, RADM2_PLACE_GLOBAL, 1, 2});
     }
     for (int sched = RADM2_SCHED_STATIC; sched <= RADM2_SCHED_PERSISTENT; sched++) {
-#define RADM2_TUNE_CAND(BS_, PL_, MB_) cands.push_back({sched, BS_, PL_, MB_});
+#define RADM2_TUNE_CAND(BS_, PL_, MB_) cands.push_back({sched, BS_, PL_, MB_, 1});
         if (c->o.parity) {
             RADM2_VARIANTS_FP64X(RADM2_TUNE_CAND)
         } else if (c->o.precision == RADM2_PREC_FP32LU) {
@@ -1158,6 +1172,7 @@ int radm2_autotune(radm2_ctx *c, double dt, const double *AbsTol, const double *
         t->o.block_threads = k.bs;
         t->o.placement = k.place;
         t->o.min_blocks = k.minb;
+        t->o.cells_per_thread = k.cpt;
         t->o.blocks_per_sm = 0;
         drop_graph(t);
         double ms = -1.0;
@@ -1227,6 +1242,7 @@ int radm2_autotune(radm2_ctx *c, double dt, const double *AbsTol, const double *
             te.block_threads = k.bs;
             te.placement = k.place;
             te.min_blocks = k.minb;
+            te.cells_per_thread = k.cpt;
             te.ms = ms[i];
             te.attempts = att[i];
         }
@@ -1245,6 +1261,7 @@ int radm2_autotune(radm2_ctx *c, double dt, const double *AbsTol, const double *
     c->o.block_threads = cands[best].bs;
     c->o.placement = cands[best].place;
     c->o.min_blocks = cands[best].minb;
+    c->o.cells_per_thread = cands[best].cpt;
     c->o.blocks_per_sm = 0;
     return RADM2_OK;
 }
@@ -1286,7 +1303,8 @@ int radm2_selfcheck(void)
     const int bad = solver_layout_check_fp64_static() | solver_layout_check_fp64_persistent() |
                     solver_layout_check_fp32_static() | solver_layout_check_fp32_persistent() |
                     solver_layout_check_fp32d_static() | solver_layout_check_fp32d_persistent() |
-                    solver_layout_check_fp64x_static() | solver_layout_check_fp64x_persistent();
+                    solver_layout_check_fp64x_static() | solver_layout_check_fp64x_persistent() |
+                    solver_layout_check_cpt2();
     return bad ? RADM2_E_STATE : RADM2_OK;
 }
 

@@ -62,6 +62,10 @@ cudaError_t launch_solver_coop_g4(const SolveArgs &a, int grid, cudaStream_t st)
 cudaError_t launch_solver_coop_g8(const SolveArgs &a, int grid, cudaStream_t st);
 cudaError_t launch_solver_coopx_g8(const SolveArgs &a, int grid, cudaStream_t st);
 
+// Two cells per thread (radm2_solver_cpt2.cuh): FP64, global placement, bs 64 or 128,
+// sched 0 static / 1 persistent.
+cudaError_t launch_solver_cpt2(const SolveArgs &a, int bs, int sched, int grid, cudaStream_t st);
+
 // Static properties of one solver variant on the current device.
 struct SolverInfo {
     int regs;           // registers per thread
@@ -93,6 +97,8 @@ cudaError_t solver_info_fp32d_static(int key, SolverInfo *out);
 cudaError_t solver_info_fp32d_persistent(int key, SolverInfo *out);
 cudaError_t solver_info_fp64x_static(int key, SolverInfo *out);
 cudaError_t solver_info_fp64x_persistent(int key, SolverInfo *out);
+cudaError_t solver_info_cpt2(int bs, int sched, SolverInfo *out);
+int solver_layout_check_cpt2();
 cudaError_t solver_info_coop_g4(SolverInfo *out);
 cudaError_t solver_info_coop_g8(SolverInfo *out);
 cudaError_t solver_info_coopx_g8(SolverInfo *out);

@@ -33,7 +33,7 @@ class Opts(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("precision", ctypes.c_int), ("refine_sweeps", ctypes.c_int),
                 ("schedule", ctypes.c_int), ("block_threads", ctypes.c_int), ("blocks_per_sm", ctypes.c_int),
                 ("float_coeffs", ctypes.c_int), ("placement", ctypes.c_int), ("min_blocks", ctypes.c_int),
-                ("parity", ctypes.c_int)]
+                ("parity", ctypes.c_int), ("cells_per_thread", ctypes.c_int)]
 
 
 class WrfGrid(ctypes.Structure):
@@ -42,7 +42,8 @@ class WrfGrid(ctypes.Structure):
 
 class TuneEntry(ctypes.Structure):
     _fields_ = [("schedule", ctypes.c_int), ("block_threads", ctypes.c_int), ("placement", ctypes.c_int),
-                ("min_blocks", ctypes.c_int), ("ms", ctypes.c_double), ("attempts", ctypes.c_longlong)]
+                ("min_blocks", ctypes.c_int), ("ms", ctypes.c_double), ("attempts", ctypes.c_longlong),
+                ("cells_per_thread", ctypes.c_int)]
 
 
 class Stats(ctypes.Structure):
@@ -204,7 +205,8 @@ class Solver:
     """One device context of the batched solver."""
 
     def __init__(self, precision=PREC_FP64, schedule=SCHED_STATIC, refine_sweeps=1, block_threads=0,
-                 blocks_per_sm=0, float_coeffs=1, device=0, placement=PLACE_GLOBAL, min_blocks=0, parity=0):
+                 blocks_per_sm=0, float_coeffs=1, device=0, placement=PLACE_GLOBAL, min_blocks=0, parity=0,
+                 cells_per_thread=1):
         self.lib = load()
         o = Opts()
         self.lib.radm2_opts_default(ctypes.byref(o))
@@ -213,6 +215,7 @@ class Solver:
         o.placement = placement
         o.min_blocks = min_blocks
         o.parity = parity
+        o.cells_per_thread = cells_per_thread
         h = ctypes.c_void_p()
         rc = self.lib.radm2_create(ctypes.byref(h), ctypes.byref(o))
         if rc != 0:

@@ -9,7 +9,7 @@ import pytest
 
 import oracle
 import radm2b200
-from conftest import ATOL, RTOL, rel_err
+from conftest import ATOL, RTOL, SAME_ARITH, rel_err
 from radm2b200 import inputs
 
 pytestmark = pytest.mark.gpu
@@ -56,14 +56,14 @@ def test_persistent_equals_static(cells4k, static_run):
     ierr, y_p, st_p, _, _, _ = run_gpu(cells4k, schedule=radm2b200.SCHED_PERSISTENT)
     assert ierr == 1
     assert np.array_equal(st_s["nacc"], st_p["nacc"])
-    assert rel_err(y_p, y_s).max() <= 1e-13
+    assert rel_err(y_p, y_s).max() <= SAME_ARITH
 
 
 @pytest.mark.parametrize("bs", [64, 256])
 def test_block_sizes(cells4k, static_run, bs):
     _, y_s, _, _, _, _ = static_run
     ierr, y, _, _, _, _ = run_gpu(cells4k, block_threads=bs, schedule=radm2b200.SCHED_PERSISTENT)
-    assert ierr == 1 and rel_err(y, y_s).max() <= 1e-13
+    assert ierr == 1 and rel_err(y, y_s).max() <= SAME_ARITH
 
 
 def test_cell_order_does_not_change_results(cells4k):
@@ -100,7 +100,7 @@ def test_split_graph_matches_loop(cells4k):
         for _ in range(3):
             ipar, rpar = radm2b200.default_params(hstart=6.0)
             assert s.rosenbrock(0.0, 600.0, ATOL, RTOL, rpar, ipar) == 1
-        assert rel_err(s.get_state(), outs[0][0]).max() <= 1e-13
+        assert rel_err(s.get_state(), outs[0][0]).max() <= SAME_ARITH
 
 
 def test_parity_full_size_subset():
@@ -249,18 +249,20 @@ def test_autotune_picks_fastest_and_keeps_results():
         y_before, acc_before = s.get_state(), int(ipar[13])
         s.set_cells(cells)
         table = s.autotune(600.0, atol, rtol, sample_cells=32768)
-        assert len(table) == 18  # 2 cooperative shapes + 8 FP64 variants x 2 schedules
+        assert len(table) == 22  # 2 cooperative shapes, 2 x 2 two-cells-per-thread, 8 FP64 variants x 2 schedules
         ran = [t for t in table if t["ms"] > 0]
         assert len(ran) >= 10 and len({t["attempts"] for t in ran}) == 1
         best = min(ran, key=lambda t: t["ms"])
         o = s.opts()
-        assert (o["schedule"], o["block_threads"], o["placement"], o["min_blocks"]) == \
-            (best["schedule"], best["block_threads"], best["placement"], best["min_blocks"])
+        assert (o["schedule"], o["block_threads"], o["placement"], o["min_blocks"], o["cells_per_thread"]) == \
+            (best["schedule"], best["block_threads"], best["placement"], best["min_blocks"], best["cells_per_thread"])
         assert np.array_equal(s.get_state(), cells["VAR"])  # the sample ran in a scratch context
         ipar, rpar = radm2b200.default_params()
         assert s.run_split(1, 600.0, atol, rtol, rpar, ipar) == 1
         assert int(ipar[13]) == acc_before
-        assert rel_err(s.get_state(), y_before).max() <= 1e-13
+        # the tuned kernel may be another instantiation (or the cooperative kernel): rounding-level
+        # differences, which the stiff cells of this mixed batch amplify to ~1e-9 at most
+        assert rel_err(s.get_state(), y_before).max() <= 1e-8
 
 
 @pytest.mark.parametrize("nchunk", [1, 5])
@@ -323,7 +325,7 @@ def test_tiny_and_odd_batches_match_oracle(n):
             ipar, rpar = radm2b200.default_params(hstart=6.0)
             assert s.rosenbrock(0.0, 600.0, atol, rtol, rpar, ipar) == 1
             ys.append(s.get_state())
-    assert rel_err(ys[1], ys[0]).max() <= 1e-13
+    assert rel_err(ys[1], ys[0]).max() <= SAME_ARITH
     ipar, rpar = radm2b200.default_params(hstart=6.0)
     ok, p = oracle.params(0.0, 600.0, atol, rtol, rpar, ipar)
     y_o, _ = oracle.integrate(cells["VAR"], cells["FIX"], rc, p)
@@ -493,3 +495,27 @@ def test_backward_window_reports_minus7_like_the_oracle(cells4k):
     ierr, y, st, ip, rp, y_o, st_o = _parity_case(sub, 600.0, 540.0, ATOL, RTOL, ipar, rpar)
     assert (st_o["status"] == -7).all()
     assert ierr == -7 and np.array_equal(st["status"], st_o["status"])
+
+
+@pytest.mark.parametrize("schedule", [radm2b200.SCHED_STATIC, radm2b200.SCHED_PERSISTENT])
+@pytest.mark.parametrize("bs", [64, 128])
+def test_two_cells_per_thread(cells4k, static_run, schedule, bs):
+    """Every thread integrating two cells side by side gives the thread-per-cell results:
+    the same arithmetic, the same per-cell step counts."""
+    _, y_s, st_s, _, ipar_s, _ = static_run
+    ierr, y, st, _, ipar, _ = run_gpu(cells4k, schedule=schedule, block_threads=bs, cells_per_thread=2)
+    assert ierr == 1 and (st["status"] == 1).all()
+    assert np.array_equal(st["nacc"], st_s["nacc"]) and np.array_equal(st["nrej"], st_s["nrej"])
+    assert rel_err(y, y_s).max() <= 1e-12
+    assert list(ipar[10:17]) == list(ipar_s[10:17])
+
+
+def test_two_cells_per_thread_odd_batch_and_options():
+    cells = inputs.make_cells(301, 17, "mixed")
+    _, y0, st0, _, _, _ = run_gpu(cells)
+    ierr, y, st, _, _, _ = run_gpu(cells, schedule=radm2b200.SCHED_PERSISTENT, cells_per_thread=2)
+    assert ierr == 1 and np.array_equal(st["nacc"], st0["nacc"]) and rel_err(y, y0).max() <= 1e-12
+    for bad in ({"precision": radm2b200.PREC_FP32LU}, {"schedule": radm2b200.SCHED_COOP}, {"parity": 1},
+                {"cells_per_thread": 3}):
+        with pytest.raises(radm2b200.RadmError):
+            radm2b200.Solver(**dict({"cells_per_thread": 2}, **bad))
