@@ -12,9 +12,9 @@
 //   error norm           each role writes the terms of its species; every role then sums
 //                        all 59 in species order (the sequential sum of mgpu.cu:3223-3238),
 //                        so every role takes the same step-control decision
-// So one cell is served by G lanes (one in each warp), and its LU (5.3 KB), state and
-// stage right-hand side live in shared memory: 32 cells x 777 words = 199 KB per block,
-// one block per SM.  The rate constants of the block's cells are copied once per cell
+// So one cell is served by G lanes (one in each warp), and its LU (5.3 KB), state, stage
+// right-hand side and RHS values live in shared memory: 32 cells x 836 words = 214 KB per
+// block, one block per SM.  The rate constants of the block's cells are copied once per cell
 // into a small per-block slot array in global memory, [156][32] per block (40 KB, L1/L2
 // resident), so that every read is a fixed offset from the lane's base address; per step
 // attempt nothing else of a cell touches global memory.
@@ -75,7 +75,8 @@ namespace radm2 {
 constexpr int COOP_LU = 0;                     // the 659 LU slots
 constexpr int COOP_Y = NJVS;                   // state Y
 constexpr int COOP_X = NJVS + NVAR;            // stage right-hand side / solution, error terms
-constexpr int COOP_DWORDS = NJVS + 2 * NVAR;   // 777
+constexpr int COOP_F = NJVS + 2 * NVAR;        // RHS values, each role its own species
+constexpr int COOP_DWORDS = NJVS + 3 * NVAR;   // 836
 // then ints
 constexpr int COOP_FLAG_LU = 0;                // [64] LU row flags
 constexpr int COOP_FLAG_SV = 64;               // [64] solve row flags
@@ -92,8 +93,9 @@ constexpr int COOP_STATUS_WAIT_LIMIT = -101;        // RADM2_E_CUDA: a wait ran 
 constexpr long long COOP_SELFTEST_WAIT_CYCLES = 1ll << 20;
 
 // Publish a finished row: every lane's stores are ordered before the flag, which one lane
-// sets once the whole warp has stored.
-__device__ __forceinline__ void coop_signal(volatile int *flag, int seq)
+// sets once the whole warp has stored.  Out of line, like coop_wait: the hundreds of call
+// sites would otherwise each carry a copy, and instruction fetch limits this kernel.
+static __device__ __noinline__ void coop_signal(volatile int *flag, int seq)
 {
     __threadfence_block();
     __syncwarp();
@@ -103,22 +105,49 @@ __device__ __forceinline__ void coop_signal(volatile int *flag, int seq)
     }
 }
 
-// Wait until another role published the row (flag >= seq), at most `limit` SM cycles.
-// After one wait has run out, later waits of the thread return at once: the block only
-// runs on to its error exit at the end of the attempt.
-__device__ __forceinline__ void coop_wait(volatile int *flag, int seq, int *werr, long long limit)
+// Wait until another role published the row (flag >= seq), at most `limit` SM cycles;
+// returns 1 if the wait ran out.  Callers skip later waits once one has run out (the block
+// then only runs on to its error exit at the end of the attempt).
+static __device__ __noinline__ int coop_wait(volatile int *flag, int seq, long long limit)
 {
-    if (*werr) return;
+    int out = 0;
     if (*flag < seq) {
         const long long t0 = clock64();
         while (*flag < seq) {
             if (clock64() - t0 > limit) {
-                *werr = 1;
+                out = 1;
                 break;
             }
         }
     }
     __threadfence_block();  // the row's loads stay after the flag
+    return out;
+}
+#define COOP_WAIT_ON(flag, seq, limit) \
+    do {                               \
+        if (!werr) werr = coop_wait((flag), (seq), (limit)); \
+    } while (0)
+
+// RHS of the role's own species at state vb (shared memory, word-major), written to fs
+// (the same layout, the role's species only).  Out of line: the step loop needs it at two
+// places (Fcn0 and the stage-2 right-hand side) and one copy of the code is enough.
+static __device__ __noinline__ void coop_fun(int role, const double *vb, const double *rcs, double fix0, double fix1,
+                                     double *fs)
+{
+    const int lane = threadIdx.x & 31;
+#define COOP_ROLE role
+#define RC(r) rcs[(r) * 32]
+#define FIX(k) ((k) == 0 ? fix0 : fix1)
+#define V(i) vb[(i) * 32 + lane]
+#define COOP_FENCE asm volatile("" ::: "memory")
+#define FUN_OUT(k, s, e) fs[(s) * 32 + lane] = (e)
+#include RADM2_COOP_FUN_INC
+#undef FUN_OUT
+#undef COOP_FENCE
+#undef V
+#undef FIX
+#undef RC
+#undef COOP_ROLE
 }
 
 __global__ void __launch_bounds__(32 * RADM2_COOP_G, 1) RADM2_COOP_KERNEL(const SolveArgs a)
@@ -128,6 +157,7 @@ __global__ void __launch_bounds__(32 * RADM2_COOP_G, 1) RADM2_COOP_KERNEL(const 
     double *const lu = smem + COOP_LU * 32;
     double *const ys = smem + COOP_Y * 32;
     double *const xs = smem + COOP_X * 32;
+    double *const fs = smem + COOP_F * 32;
     int *const ism = reinterpret_cast<int *>(smem + COOP_DWORDS * 32);
     volatile int *const vflag = ism;
     const int lane = threadIdx.x & 31;
@@ -230,15 +260,11 @@ __global__ void __launch_bounds__(32 * RADM2_COOP_G, 1) RADM2_COOP_KERNEL(const 
 
         // ================================================================ Fcn0 = F(Y)
         if (__syncthreads_or(outer)) {
-            double fo[NS];
-#define V(i) SW(ys, i)
-#define FUN_OUT(k, e) fo[k] = (e)
-#include RADM2_COOP_FUN_INC
-#undef FUN_OUT
-#undef V
-#pragma unroll
-            for (int k = 0; k < NS; k++)
-                if (outer) f0[k] = fo[k];
+            coop_fun(role, ys, rcs, fix0, fix1, fs);
+#define OWN(k, s) \
+    if (outer) f0[k] = SW(fs, s);
+#include RADM2_COOP_OWN_INC
+#undef OWN
         }
         outer = false;
 
@@ -276,13 +302,13 @@ __global__ void __launch_bounds__(32 * RADM2_COOP_G, 1) RADM2_COOP_KERNEL(const 
         // LU, rows split between the roles
         lu_seq++;
         if (a.coop_selftest && role == 1)  // a flag nothing sets: the bounded wait runs out
-            coop_wait(vflag + COOP_FLAG_NEVER, lu_seq, &werr, COOP_SELFTEST_WAIT_CYCLES);
+            COOP_WAIT_ON(vflag + COOP_FLAG_NEVER, lu_seq, COOP_SELFTEST_WAIT_CYCLES);
         {
 #define G(s) SW(lu, s)
 #define LU_T double
 #define LU_PIVOT_CHECK(k, v) \
     if ((v) == 0.0) ism[COOP_SING + lane] = 1
-#define LU_WAIT(j) coop_wait(vflag + COOP_FLAG_LU + (j), lu_seq, &werr, COOP_WAIT_CYCLES)
+#define LU_WAIT(j) COOP_WAIT_ON(vflag + COOP_FLAG_LU + (j), lu_seq, COOP_WAIT_CYCLES)
 #define LU_DONE(i) coop_signal(vflag + COOP_FLAG_LU + (i), lu_seq)
 #include RADM2_COOP_LU_INC
 #undef LU_WAIT
@@ -314,17 +340,13 @@ __global__ void __launch_bounds__(32 * RADM2_COOP_G, 1) RADM2_COOP_KERNEL(const 
 #include RADM2_COOP_OWN_INC
 #undef OWN
                 __syncthreads();
-                double fo[NS];
-#define V(i) SW(xs, i)
-#define FUN_OUT(k, e) fo[k] = (e)
-#include RADM2_COOP_FUN_INC
-#undef FUN_OUT
-#undef V
+                coop_fun(role, xs, rcs, fix0, fix1, fs);
                 __syncthreads();  // every role has read Y + A21 K1
-#define OWN(k, s)                          \
-    {                                      \
-        SW(xs, s) = fo[k] + k1[k] * hc21;  \
-        k3[k] = fo[k] + k1[k] * hc31;      \
+#define OWN(k, s)                              \
+    {                                          \
+        const double f = SW(fs, s);            \
+        SW(xs, s) = f + k1[k] * hc21;          \
+        k3[k] = f + k1[k] * hc31;              \
     }
 #include RADM2_COOP_OWN_INC
 #undef OWN
@@ -342,7 +364,7 @@ __global__ void __launch_bounds__(32 * RADM2_COOP_G, 1) RADM2_COOP_KERNEL(const 
             // forward rows (flags), barrier, backward rows (flags), barrier
 #define G(s) SW(lu, s)
 #define X(i) SW(xs, i)
-#define SOLVE_WAIT(j) coop_wait(vflag + COOP_FLAG_SV + (j), sv_seq, &werr, COOP_WAIT_CYCLES)
+#define SOLVE_WAIT(j) COOP_WAIT_ON(vflag + COOP_FLAG_SV + (j), sv_seq, COOP_WAIT_CYCLES)
 #define SOLVE_DONE(i) coop_signal(vflag + COOP_FLAG_SV + (i), sv_seq)
             sv_seq++;
 #include RADM2_COOP_FWD_INC

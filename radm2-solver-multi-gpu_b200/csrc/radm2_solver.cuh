@@ -269,7 +269,12 @@ __device__ RADM2_PHASE void ph_stage(int stage, const double *y, const double *r
 #undef G
 }
 
-template <int BS, typename LUT, int SCHED, int PLACE, int MINB, int IR = 1>
+// ARITH tags the arithmetic the including file compiles the kernel with (0 = the fast form,
+// 1 = reference arithmetic: RADM2_LU_RECIP=0 and no multiply-add contraction).  The body does
+// not read it; it makes the two forms distinct instantiations, so that the same (BS, LUT,
+// SCHED, PLACE, MINB) built both ways in two files are two kernels, not one name with two
+// definitions.
+template <int BS, typename LUT, int SCHED, int PLACE, int MINB, int IR = 1, int ARITH = 0>
 __global__ void __launch_bounds__(BS, MINB) k_rosenbrock(const SolveArgs a)
 {
     using L = Layout<LUT, PLACE>;

@@ -1,6 +1,7 @@
 // Instantiations of the fused solver kernel in reference arithmetic (radm2_opts.parity):
 // fp64 LU with the pivot divisions kept, built without multiply-add contraction
 // (Makefile: -DRADM2_LU_RECIP=0 --fmad=false), static schedule.
+#define RADM2_ARITH 1
 #include "radm2_solver_inst.h"
 
 #define RADM2_T double

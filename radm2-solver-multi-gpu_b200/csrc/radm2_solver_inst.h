@@ -8,10 +8,10 @@
 
 namespace radm2 {
 
-template <int BS, typename LUT, int SCHED, int PLACE, int MINB, int IR>
+template <int BS, typename LUT, int SCHED, int PLACE, int MINB, int IR, int ARITH>
 cudaError_t launch_one(const SolveArgs &a, int grid, cudaStream_t st)
 {
-    auto k = k_rosenbrock<BS, LUT, SCHED, PLACE, MINB, IR>;
+    auto k = k_rosenbrock<BS, LUT, SCHED, PLACE, MINB, IR, ARITH>;
     const size_t smem = (size_t)Layout<LUT, PLACE>::smem_words * sizeof(double) * BS;
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -22,10 +22,10 @@ cudaError_t launch_one(const SolveArgs &a, int grid, cudaStream_t st)
     return cudaGetLastError();
 }
 
-template <int BS, typename LUT, int SCHED, int PLACE, int MINB, int IR>
+template <int BS, typename LUT, int SCHED, int PLACE, int MINB, int IR, int ARITH>
 cudaError_t info_one(SolverInfo *out)
 {
-    auto k = k_rosenbrock<BS, LUT, SCHED, PLACE, MINB, IR>;
+    auto k = k_rosenbrock<BS, LUT, SCHED, PLACE, MINB, IR, ARITH>;
     const size_t smem = (size_t)Layout<LUT, PLACE>::smem_words * sizeof(double) * BS;
     cudaFuncAttributes at{};
     cudaError_t e = cudaFuncGetAttributes(&at, k);
@@ -59,12 +59,16 @@ int check_one()
 #ifndef RADM2_IR
 #define RADM2_IR 1
 #endif
+// 1 in the files built in reference arithmetic (see k_rosenbrock's ARITH)
+#ifndef RADM2_ARITH
+#define RADM2_ARITH 0
+#endif
 
 #define RADM2_KEY(BS_, PL_, MB_) ((BS_) * 64 + (MB_) * 4 + (PL_))
 #define RADM2_CASE_LAUNCH(BS_, PL_, MB_) \
-    case RADM2_KEY(BS_, PL_, MB_): return launch_one<BS_, RADM2_T, RADM2_S, PL_, MB_, RADM2_IR>(a, grid, st);
+    case RADM2_KEY(BS_, PL_, MB_): return launch_one<BS_, RADM2_T, RADM2_S, PL_, MB_, RADM2_IR, RADM2_ARITH>(a, grid, st);
 #define RADM2_CASE_INFO(BS_, PL_, MB_) \
-    case RADM2_KEY(BS_, PL_, MB_): return info_one<BS_, RADM2_T, RADM2_S, PL_, MB_, RADM2_IR>(out);
+    case RADM2_KEY(BS_, PL_, MB_): return info_one<BS_, RADM2_T, RADM2_S, PL_, MB_, RADM2_IR, RADM2_ARITH>(out);
 #define RADM2_CHECK(BS_, PL_, MB_) bad |= check_one<BS_, RADM2_T, RADM2_S, PL_, MB_>();
 
 #define RADM2_DEFINE_SOLVER(NAME, LIST)                                                                  \

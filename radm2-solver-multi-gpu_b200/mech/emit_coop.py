@@ -10,7 +10,7 @@ registers.  This module decides the split and writes it out as fragments:
   radm2_coop_g<G>_own.inc    species owned by each role (stage vectors, error terms):
                              OWN(k, species) per owned species, k = register slot
   radm2_coop_g<G>_fun.inc    RHS of the owned species, reference association order
-                             (mgpu.cu:1103-1385): FUN_OUT(k, value)
+                             (mgpu.cu:1103-1385): FUN_OUT(k, species, value)
   radm2_coop_g<G>_jac.inc    Jacobian slots of the role, G = -J (+ ghinv on the diagonal):
                              JAC_OUT / JAC_OUT_DIAG / JAC_OUT_ZERO (mgpu.cu:1685-2652)
   radm2_coop_g<G>_lu.inc     LU rows of the role (row-Doolittle blocks of mgpu.cu:2746-2779),
@@ -205,7 +205,8 @@ def emit_role_code(m, G, out_dir):
             assert len(rs) == 1, (i, term)
             uses.setdefault(rs.pop(), []).append((i, pos, op, term))
     body = [banner, "/* RHS of each role's species, mgpu.cu:1103-1385, reaction-major (bit-identical to the\n"
-            " * reference's sums).  Inputs: RC(r), V(i), FIX(k).  Output FUN_OUT(k, value) for owned slot k. */\n",
+            " * reference's sums).  Inputs: RC(r), V(i), FIX(k).  Output FUN_OUT(k, species, value) for owned\n"
+            " * slot k. */\n",
             "switch (COOP_ROLE) {\n"]
     for ro in range(G):
         body.append("case %d: {\n" % ro)
@@ -228,7 +229,7 @@ def emit_role_code(m, G, out_dir):
                     body.append("    vd%d = (vd%d %s %s);\n" % (i, i, op, r(term)))
             body.append("  }\n")
         for s_ in own[ro]:
-            body.append("  FUN_OUT(%d, vd%d);\n" % (slot[s_], s_))
+            body.append("  FUN_OUT(%d, %d, vd%d);\n" % (slot[s_], s_, s_))
         body.append("} break;\n")
     body.append("default: break;\n}\n")
     emit.write(os.path.join(out_dir, "radm2_coop_g%d_fun.inc" % G), body)

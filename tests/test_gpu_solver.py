@@ -260,9 +260,9 @@ def test_autotune_picks_fastest_and_keeps_results():
         ipar, rpar = radm2b200.default_params()
         assert s.run_split(1, 600.0, atol, rtol, rpar, ipar) == 1
         assert int(ipar[13]) == acc_before
-        # the tuned kernel may be another instantiation (or the cooperative kernel): rounding-level
-        # differences, which the stiff cells of this mixed batch amplify to ~1e-9 at most
-        assert rel_err(s.get_state(), y_before).max() <= 1e-8
+        # the tuned kernel may have another code shape (cooperative, two cells per thread):
+        # differently contracted multiply-adds, amplified in this mixed batch's stiff cells
+        assert rel_err(s.get_state(), y_before).max() <= 1e-10
 
 
 @pytest.mark.parametrize("nchunk", [1, 5])
@@ -506,6 +506,7 @@ def test_two_cells_per_thread(cells4k, static_run, schedule, bs):
     ierr, y, st, _, ipar, _ = run_gpu(cells4k, schedule=schedule, block_threads=bs, cells_per_thread=2)
     assert ierr == 1 and (st["status"] == 1).all()
     assert np.array_equal(st["nacc"], st_s["nacc"]) and np.array_equal(st["nrej"], st_s["nrej"])
+    # the same expressions in another code shape: differently contracted multiply-adds
     assert rel_err(y, y_s).max() <= 1e-12
     assert list(ipar[10:17]) == list(ipar_s[10:17])
 
@@ -514,7 +515,8 @@ def test_two_cells_per_thread_odd_batch_and_options():
     cells = inputs.make_cells(301, 17, "mixed")
     _, y0, st0, _, _, _ = run_gpu(cells)
     ierr, y, st, _, _, _ = run_gpu(cells, schedule=radm2b200.SCHED_PERSISTENT, cells_per_thread=2)
-    assert ierr == 1 and np.array_equal(st["nacc"], st0["nacc"]) and rel_err(y, y0).max() <= 1e-12
+    # a mixed batch: its stiff cells amplify the rounding-level differences
+    assert ierr == 1 and np.array_equal(st["nacc"], st0["nacc"]) and rel_err(y, y0).max() <= 1e-10
     for bad in ({"precision": radm2b200.PREC_FP32LU}, {"schedule": radm2b200.SCHED_COOP}, {"parity": 1},
                 {"cells_per_thread": 3}):
         with pytest.raises(radm2b200.RadmError):

@@ -5,10 +5,9 @@ all of the GPU's memory for its own pool at start-up, or a coupling whose device
 budget is fixed at initialisation.  This test allocates the caller's input/output buffers
 itself (the caller owns those), calls the entry point through the C ABI several times in a
 row, and checks each result against the context-based radm2_rosenbrock on the same cells and
-against the CPU oracle.  Against the context entry point (same solver kernel) the results
-must agree to rounding level; against the oracle within 1e-9 relative (floor 1 molec/cm^3):
-the no-alloc call runs the fast solver (reciprocal pivots, contracted multiply-adds), whose
-deviation from the oracle reaches a few 1e-10 in stiff cells.  It also checks with cudaMemGetInfo that a call after the
+against the CPU oracle: to 1e-13 relative against the context entry point running the same
+solver kernel, and within the parity tolerance the other solver tests use against the oracle
+(1e-10 relative, floor 1 molec/cm^3).  It also checks with cudaMemGetInfo that a call after the
 first (the set-up call) leaves the device's free memory unchanged.  The file is collected
 last on purpose; it passes alone in a fresh process and after the others.
 """
@@ -23,7 +22,7 @@ from conftest import ATOL, RTOL, SAME_ARITH, rel_err
 from radm2b200 import inputs
 
 pytestmark = pytest.mark.gpu
-FAST_VS_ORACLE = 1e-9
+PARITY = 1e-10
 MAX_CELLS = 32768
 
 
@@ -118,7 +117,7 @@ def test_noalloc_matches_context_entry_point_and_oracle_without_allocating():
         assert ierr == 1, (k, ierr)
         assert (st == 1).all() and (st == st_ref).all()
         assert rel_err(y, y_ref).max() <= SAME_ARITH, k
-        assert rel_err(y, y_orc).max() <= FAST_VS_ORACLE, k
+        assert rel_err(y, y_orc).max() <= PARITY, k
         assert list(ipar[10:17]) == list(ipar_ref[10:17])
         assert rpar[10] == rpar_ref[10] == 600.0 and abs(rpar[11] - rpar_ref[11]) <= 1e-12 * rpar_ref[11]
     torch.cuda.synchronize()
@@ -145,7 +144,7 @@ def test_noalloc_without_status_array_at_the_size_limit():
         assert list(ipar[10:17]) == list(ipar_ref[10:17])
         assert abs(rpar[11] - rpar_ref[11]) <= 1e-12 * rpar_ref[11]
     idx = np.arange(0, MAX_CELLS, 64)
-    assert rel_err(y[idx], _oracle(cells, rc, idx)).max() <= FAST_VS_ORACLE
+    assert rel_err(y[idx], _oracle(cells, rc, idx)).max() <= PARITY
 
 
 def test_noalloc_rejects_oversize_and_bad_parameters():
