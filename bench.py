@@ -95,6 +95,8 @@ def parse():
                     help="skip the arms timed at the loosest rtol that meets the metric's 1e-3 accuracy gate")
     ap.add_argument("--gate-steps", type=int, default=3,
                     help="consecutive splits timed by each accuracy-gated arm (tight tolerances take many steps)")
+    ap.add_argument("--split-stats", action="store_true",
+                    help="report accepted/rejected steps of each timed split (replayed untimed afterwards)")
     ap.add_argument("--parity", action="store_true",
                     help="time the reference-arithmetic FP64 solver (divisions kept, no multiply-add contraction)")
     return ap.parse_args()
@@ -393,6 +395,15 @@ def main():
     value = ncell * world * args.steps / (main_arm["el_ms"] * 1e-3)
     y_main = solver.get_state() if rank == 0 else None
     tuned_opts = solver.opts()
+    split_stats = None
+    if args.split_stats:  # the timed splits again, one at a time (untimed): attempts per split
+        solver.set_state_device(main_arm["y0"].data_ptr(), ld)
+        split_stats = []
+        for _ in range(args.steps):
+            ipar, rpar = radm2b200.default_params()
+            assert solver.run_split(1, dt, atol, rtol, rpar, ipar) == 1
+            st = solver.stats()
+            split_stats.append([st["n_accepted"], st["n_rejected"]])
 
     # ---- end to end through the C ABI with host buffers (pinned), same method
     e2e = None
@@ -624,6 +635,8 @@ def main():
         line["accuracy"] = accuracy
     if gated is not None:
         line["at_accuracy_gate"] = gated
+    if split_stats is not None:
+        line["attempts_per_split"] = split_stats
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cells, dt, args.steps)
     print(json.dumps(line), flush=True)

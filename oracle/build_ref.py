@@ -24,7 +24,9 @@ tables recovered from dev_KppSolve -- the reference never fills its own).
 Outputs go to oracle/_ref/ only (git-ignored; the built .so travels with the
 repository snapshot to machines that have no copy of the reference).
 
-Usage:  python oracle/build_ref.py [/path/to/mgpu.cu]
+Usage:  python oracle/build_ref.py /path/to/mgpu.cu
+        (or the path in the environment variable RADM2_REFERENCE_MGPU; without either, or
+        when the file is absent, nothing is built and a prebuilt oracle/_ref is kept)
 """
 import os
 import re
@@ -33,7 +35,6 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
-DEFAULT_SRC = "/root/reference/mgpu.cu"
 
 FUNCTIONS = [
     r"__device__\s+double\s+ARR2\s*\(",
@@ -73,8 +74,8 @@ def function_text(src, signature):
 
 
 def main():
-    src_path = sys.argv[1] if len(sys.argv) > 1 else DEFAULT_SRC
-    if not os.path.exists(src_path):
+    src_path = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("RADM2_REFERENCE_MGPU", "")
+    if not src_path or not os.path.exists(src_path):
         print("reference not present (%s); keeping any prebuilt oracle/_ref" % src_path)
         return 0
     with open(src_path) as f:

@@ -18,7 +18,7 @@ it with exactly the reference's association order; nothing is simplified.
 The output, mech/radm2_mech.json, is committed: the build and the GPU runs do
 not need the reference.
 
-Usage:  python gen_mech.py [/path/to/mgpu.cu]   (default /root/reference/mgpu.cu)
+Usage:  python gen_mech.py /path/to/mgpu.cu
 """
 import ast
 import json
@@ -27,7 +27,6 @@ import re
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-DEFAULT_SRC = "/root/reference/mgpu.cu"
 
 # Expected LU structure of the RADM2 mechanism (row starts and diagonal slots).
 EXPECT_CROW = [0, 3, 9, 26, 29, 31, 33, 35, 37, 39, 41, 43, 46, 49, 52, 55, 57, 62, 66, 71, 75, 79,
@@ -212,7 +211,9 @@ def check_closed(pattern):
 
 
 def main():
-    src_path = sys.argv[1] if len(sys.argv) > 1 else DEFAULT_SRC
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: python gen_mech.py /path/to/mgpu.cu")
+    src_path = sys.argv[1]
     with open(src_path) as f:
         src = f.read()
 
