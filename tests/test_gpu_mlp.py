@@ -72,8 +72,13 @@ def test_gradients_match_reference(feats):
 
 def test_training_reduces_loss_and_gains_steps():
     """Train on traces of one seed, evaluate on a disjoint seed: seeded starting steps must
-    cut the step attempts of the same integration, and the answers stay as accurate as the
-    unseeded method's against an FP64 oracle run at rtol 1e-8 (checked on a subset)."""
+    cut the step attempts of the same integration.  Accuracy against an FP64 rtol 1e-8
+    reference (GPU, atol 1e-4; 16 of its cells re-checked by the CPU oracle), on every entry
+    above 1 molec/cm^3: the seeded run's 99.9th-percentile error may exceed the unseeded
+    run's by at most 10%.  Its largest single error is printed and bounded loosely (1.5x):
+    the seeded first step of each split sits nearer the controller's tolerance, and the
+    maximum over ~480k entries is one stiff cell's species; bench.py compares the two
+    methods at equal accuracy instead."""
     import oracle
     X, Y = seeding.generate_traces(32768, 3, seed=101)
     net, hist = seeding.fit(X, Y, epochs=12, batch=1024, lr=3e-3)
@@ -85,21 +90,29 @@ def test_training_reduces_loss_and_gains_steps():
     print("attempts default %d learned %d (accepted %d -> %d, rejected %d -> %d)"
           % (att0, att1, t0["acc"], t1["acc"], t0["rej"], t1["rej"]))
     assert att1 < att0
-    # accuracy against a tight oracle on 96 cells: the seeded run is no worse than the default
-    idx = np.arange(0, 8192, 86)[:96]
-    with radm2b200.Solver() as s:
+    tight_atol, tight_rtol = np.full(59, 1e-4), np.full(59, 1e-8)
+    with radm2b200.Solver(schedule=radm2b200.SCHED_PERSISTENT) as s:
         s.set_cells(cells)
-        rc = s.get_rconst()[idx]
+        s.update_rconst()
+        rc = s.get_rconst()
+        ipar, rpar = radm2b200.default_params()
+        assert s.run_split(3, 600.0, tight_atol, tight_rtol, rpar, ipar, use_graph=False) == 1
+        yt = s.get_state()
+    idx = np.arange(0, 8192, 512)
     ipar, rpar = radm2b200.default_params(hstart=6.0)
-    ok, p = oracle.params(0.0, 600.0, np.ones(59), np.full(59, 1e-8), rpar, ipar)
-    yt = cells["VAR"][idx]
+    ok, p = oracle.params(0.0, 600.0, tight_atol, tight_rtol, rpar, ipar)
+    yo = cells["VAR"][idx]
     for _ in range(3):
-        yt, _ = oracle.integrate(yt, cells["FIX"][idx], rc, p)
+        yo, _ = oracle.integrate(yo, cells["FIX"][idx], rc[idx], p)
+    assert (np.abs(yt[idx] - yo) / np.maximum(np.abs(yo), 1.0)).max() <= 1e-9
     above = np.abs(yt) > 1.0
-    e0 = (np.abs(y0[idx] - yt)[above] / np.abs(yt)[above]).max()
-    e1 = (np.abs(y1[idx] - yt)[above] / np.abs(yt)[above]).max()
-    print("max rel err vs rtol-1e-8 oracle: default %.2e learned %.2e" % (e0, e1))
-    assert e1 <= 1.5 * e0 + 1e-3
+    e0 = np.abs(y0 - yt)[above] / np.abs(yt)[above]
+    e1 = np.abs(y1 - yt)[above] / np.abs(yt)[above]
+    q0, q1 = np.quantile(e0, 0.999), np.quantile(e1, 0.999)
+    print("rel err vs rtol-1e-8 reference: p99.9 default %.2e learned %.2e; max default %.2e learned %.2e"
+          % (q0, q1, e0.max(), e1.max()))
+    assert q1 <= 1.1 * q0
+    assert e1.max() <= 1.5 * e0.max()
 
 
 def test_attached_seeding_in_graph_matches_host_driven():
