@@ -50,9 +50,8 @@ extern "C" {
 #define RADM2_SCHED_COOP 2       /* cooperative: 32 cells per block with the whole working set
                                     (LU, state, stage vectors) on chip; the block's warps split
                                     every phase of a step between them, so each cell is served
-                                    by one lane in each warp; block_threads 128, 256 (default)
-                                    or 512: 4, 8 or 16 warps per group of 32 cells; FP64;
-                                    cells from a work queue */
+                                    by one lane in each warp; block_threads 128 (4 warps per cell
+                                    group) or 256 (8, default); FP64; cells from a work queue */
 
 typedef struct radm2_opts {
     int device;         /* CUDA device ordinal (default 0) */

@@ -255,10 +255,7 @@ cudaError_t variant_info(radm2_ctx *c, int bs, SolverInfo *info)
     if (c->o.cells_per_thread == 2) return solver_info_cpt2(bs, c->o.schedule, info);
     if (c->o.schedule == RADM2_SCHED_COOP) {
         if (c->o.parity) return bs == 256 ? solver_info_coopx_g8(info) : cudaErrorInvalidValue;
-        return bs == 128 ? solver_info_coop_g4(info)
-               : bs == 256 ? solver_info_coop_g8(info)
-               : bs == 512 ? solver_info_coop_g16(info)
-                           : cudaErrorInvalidValue;
+        return bs == 128 ? solver_info_coop_g4(info) : bs == 256 ? solver_info_coop_g8(info) : cudaErrorInvalidValue;
     }
     const bool fp32 = c->o.precision == RADM2_PREC_FP32LU;
     const bool pers = c->o.schedule == RADM2_SCHED_PERSISTENT;
@@ -357,9 +354,7 @@ cudaError_t launch_solver(radm2_ctx *c, const SolveArgs &a, int bs, int grid)
     if (c->o.cells_per_thread == 2) return launch_solver_cpt2(a, bs, c->o.schedule, grid, c->st);
     if (c->o.schedule == RADM2_SCHED_COOP) {
         if (c->o.parity) return launch_solver_coopx_g8(a, grid, c->st);
-        return bs == 128 ? launch_solver_coop_g4(a, grid, c->st)
-               : bs == 512 ? launch_solver_coop_g16(a, grid, c->st)
-                           : launch_solver_coop_g8(a, grid, c->st);
+        return bs == 128 ? launch_solver_coop_g4(a, grid, c->st) : launch_solver_coop_g8(a, grid, c->st);
     }
     if (c->o.parity)  // reference arithmetic: divisions kept, no multiply-add contraction
         return pers ? launch_solver_fp64x_persistent(a, k, grid, c->st) : launch_solver_fp64x_static(a, k, grid, c->st);
@@ -510,9 +505,6 @@ int radm2_create(radm2_ctx **out, const radm2_opts *opts)
         return RADM2_E_ARG;
     if (o.parity && (o.precision != RADM2_PREC_FP64 || o.placement != RADM2_PLACE_GLOBAL)) return RADM2_E_ARG;
     int ndev = 0;
-    if (o.schedule == RADM2_SCHED_COOP && o.block_threads && o.block_threads != 128 && o.block_threads != 256 &&
-        o.block_threads != 512)
-        return RADM2_E_ARG;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= o.device || o.device < 0) return RADM2_E_NODEV;
     cudaDeviceProp prop;
     if (cudaGetDeviceProperties(&prop, o.device) != cudaSuccess) return RADM2_E_NODEV;
@@ -1125,7 +1117,6 @@ int radm2_autotune(radm2_ctx *c, double dt, const double *AbsTol, const double *
     if (c->o.precision == RADM2_PREC_FP64) {  // cooperative blocks: 4 or 8 warps per 32 cells
         if (!c->o.parity) cands.push_back({RADM2_SCHED_COOP, 128, RADM2_PLACE_GLOBAL, 1, 1});
         cands.push_back({RADM2_SCHED_COOP, 256, RADM2_PLACE_GLOBAL, 1, 1});
-        if (!c->o.parity) cands.push_back({RADM2_SCHED_COOP, 512, RADM2_PLACE_GLOBAL, 1, 1});
         if (!c->o.parity)  // two cells per thread
             for (int sched = RADM2_SCHED_STATIC; sched <= RADM2_SCHED_PERSISTENT; sched++)
                 for (int bs : {64, 128}) cands.push_back({sched, bs, RADM2_PLACE_GLOBAL, 1, 2});

@@ -29,7 +29,7 @@
 // hanging the GPU.
 //
 // This header is included by one instantiation file per kernel, which defines
-//   RADM2_COOP_G       roles (warps) per block: 4, 8 or 16
+//   RADM2_COOP_G       roles (warps) per block: 4 or 8
 //   RADM2_COOP_RECIP   1 = reciprocal pivots (the fast form), 0 = the reference's divisions
 //                      (that file is compiled without multiply-add contraction)
 //   RADM2_COOP_KERNEL  the kernel's name
@@ -65,22 +65,8 @@
 #define RADM2_COOP_LU_INC "gen/radm2_coop_g8_lu_div.inc"
 #define RADM2_COOP_BWD_INC "gen/radm2_coop_g8_bwd_div.inc"
 #endif
-#elif RADM2_COOP_G == 16
-#include "gen/radm2_coop_g16.h"
-#define RADM2_COOP_NS RADM2_COOP_G16_NS
-#define RADM2_COOP_OWN_INC "gen/radm2_coop_g16_own.inc"
-#define RADM2_COOP_FUN_INC "gen/radm2_coop_g16_fun.inc"
-#define RADM2_COOP_JAC_INC "gen/radm2_coop_g16_jac.inc"
-#define RADM2_COOP_FWD_INC "gen/radm2_coop_g16_fwd.inc"
-#if RADM2_COOP_RECIP
-#define RADM2_COOP_LU_INC "gen/radm2_coop_g16_lu.inc"
-#define RADM2_COOP_BWD_INC "gen/radm2_coop_g16_bwd.inc"
 #else
-#define RADM2_COOP_LU_INC "gen/radm2_coop_g16_lu_div.inc"
-#define RADM2_COOP_BWD_INC "gen/radm2_coop_g16_bwd_div.inc"
-#endif
-#else
-#error "RADM2_COOP_G must be 4, 8 or 16"
+#error "RADM2_COOP_G must be 4 or 8"
 #endif
 
 namespace radm2 {

@@ -60,7 +60,6 @@ cudaError_t launch_reduce(int n, const int *status, const int *nacc, const int *
 // one block per SM; the "x" kernel keeps the reference's arithmetic.
 cudaError_t launch_solver_coop_g4(const SolveArgs &a, int grid, cudaStream_t st);
 cudaError_t launch_solver_coop_g8(const SolveArgs &a, int grid, cudaStream_t st);
-cudaError_t launch_solver_coop_g16(const SolveArgs &a, int grid, cudaStream_t st);
 cudaError_t launch_solver_coopx_g8(const SolveArgs &a, int grid, cudaStream_t st);
 
 // Two cells per thread (radm2_solver_cpt2.cuh): FP64, global placement, bs 64 or 128,
@@ -102,7 +101,6 @@ cudaError_t solver_info_cpt2(int bs, int sched, SolverInfo *out);
 int solver_layout_check_cpt2();
 cudaError_t solver_info_coop_g4(SolverInfo *out);
 cudaError_t solver_info_coop_g8(SolverInfo *out);
-cudaError_t solver_info_coop_g16(SolverInfo *out);
 cudaError_t solver_info_coopx_g8(SolverInfo *out);
 // Host-side bounds check of every built variant's working-set layout (0 = all in bounds).
 int solver_layout_check_fp64_static();

@@ -38,7 +38,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 import emit  # noqa: E402
 
-ROLE_COUNTS = (4, 8, 16)
+ROLE_COUNTS = (4, 8)
 
 # Cost model (SM cycles) for the list scheduler.
 C_LOAD = 2        # one shared-memory load issued (32 lanes x 8 B = 2 wavefronts)
