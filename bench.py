@@ -97,7 +97,7 @@ def parse():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain comparison arm")
     ap.add_argument("--ref-step-seconds", type=float, default=8.0,
                     help="reference arm: size each step's CPU sample to about this long")
-    ap.add_argument("--e2e-chunks", type=int, default=4,
+    ap.add_argument("--e2e-chunks", type=int, default=8,
                     help="e2e: chunks of the pipelined host-buffer call (0 = separate set/run/get calls)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")

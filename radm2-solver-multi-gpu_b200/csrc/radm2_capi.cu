@@ -346,24 +346,23 @@ SolveArgs make_args(radm2_ctx *c, const SolveParams &p, int *queue)
     return a;
 }
 
-cudaError_t launch_solver(radm2_ctx *c, const SolveArgs &a, int bs, int grid, cudaStream_t stream = nullptr)
+cudaError_t launch_solver(radm2_ctx *c, const SolveArgs &a, int bs, int grid)
 {
-    cudaStream_t st = stream ? stream : c->st;
     const bool fp32 = c->o.precision == RADM2_PREC_FP32LU;
     const bool pers = c->o.schedule == RADM2_SCHED_PERSISTENT;
     const int k = key_of(c, bs);
-    if (c->o.cells_per_thread == 2) return launch_solver_cpt2(a, bs, c->o.schedule, grid, st);
+    if (c->o.cells_per_thread == 2) return launch_solver_cpt2(a, bs, c->o.schedule, grid, c->st);
     if (c->o.schedule == RADM2_SCHED_COOP) {
-        if (c->o.parity) return launch_solver_coopx_g8(a, grid, st);
-        return bs == 128 ? launch_solver_coop_g4(a, grid, st) : launch_solver_coop_g8(a, grid, st);
+        if (c->o.parity) return launch_solver_coopx_g8(a, grid, c->st);
+        return bs == 128 ? launch_solver_coop_g4(a, grid, c->st) : launch_solver_coop_g8(a, grid, c->st);
     }
     if (c->o.parity)  // reference arithmetic: divisions kept, no multiply-add contraction
-        return pers ? launch_solver_fp64x_persistent(a, k, grid, st) : launch_solver_fp64x_static(a, k, grid, st);
+        return pers ? launch_solver_fp64x_persistent(a, k, grid, c->st) : launch_solver_fp64x_static(a, k, grid, c->st);
     if (fp32 && c->o.refine_sweeps == 0)  // the variants without the refinement code
-        return pers ? launch_solver_fp32d_persistent(a, k, grid, st) : launch_solver_fp32d_static(a, k, grid, st);
+        return pers ? launch_solver_fp32d_persistent(a, k, grid, c->st) : launch_solver_fp32d_static(a, k, grid, c->st);
     if (fp32)
-        return pers ? launch_solver_fp32_persistent(a, k, grid, st) : launch_solver_fp32_static(a, k, grid, st);
-    return pers ? launch_solver_fp64_persistent(a, k, grid, st) : launch_solver_fp64_static(a, k, grid, st);
+        return pers ? launch_solver_fp32_persistent(a, k, grid, c->st) : launch_solver_fp32_static(a, k, grid, c->st);
+    return pers ? launch_solver_fp64_persistent(a, k, grid, c->st) : launch_solver_fp64_static(a, k, grid, c->st);
 }
 
 // Record a kernel-timing event.  Under stream capture the External flag makes the record
@@ -549,9 +548,6 @@ int radm2_destroy(radm2_ctx *c)
     for (cudaEvent_t e : c->pipe_ev) cudaEventDestroy(e);
     if (c->st_up) cudaStreamDestroy(c->st_up);
     if (c->st_down) cudaStreamDestroy(c->st_down);
-    if (c->st_c2) cudaStreamDestroy(c->st_c2);
-    if (c->scratch2) cudaFree(c->scratch2);
-    if (c->partials2) cudaFree(c->partials2);
     if (c->own) cudaStreamDestroy(c->own);
     delete c;
     return RADM2_OK;
@@ -733,10 +729,8 @@ int radm2_rosenbrock(radm2_ctx *c, double Tstart, double Tend, const double *Abs
 // Host-buffer integration with the transfers hidden behind the solve: the batch is cut into
 // nchunk consecutive chunks.  Chunk k's inputs go up (copy stream, then a transpose to the
 // struct-of-arrays arrays) while chunk k-1 integrates (rate constants, optional seeding,
-// solver, statistics) and chunk k-2's states come back (transpose and copy on a second copy
-// stream).  Even chunks integrate on the context's stream, odd ones on a second compute
-// stream with their own solver scratch, so a chunk's solver launch takes the SMs that the
-// previous chunk's tail of slow cells leaves idle.  Events order each chunk's three steps.
+// solver, statistics on the context's stream) and chunk k-2's states come back (transpose
+// and copy on a second copy stream).  Events order each chunk's three steps.
 int radm2_rosenbrock_host(radm2_ctx *c, int ncell, double *VAR, const double *FIX, const double *TEMP,
                           const double *RC_N2O5, const double *JV, double Tstart, double Tend, const double *AbsTol,
                           const double *RelTol, double *RPAR, int *IPAR, int nchunk)
@@ -766,19 +760,6 @@ int radm2_rosenbrock_host(radm2_ctx *c, int ncell, double *VAR, const double *FI
     double *sv = c->stage, *sf = sv + n * NVAR, *st_ = sf + n * NFIX, *sr = st_ + n, *sj = sr + n, *so = sj + n * NPH;
     if (!c->st_up) CK(cudaStreamCreateWithFlags(&c->st_up, cudaStreamNonBlocking));
     if (!c->st_down) CK(cudaStreamCreateWithFlags(&c->st_down, cudaStreamNonBlocking));
-    // Odd chunks integrate on a second compute stream with their own solver scratch and
-    // statistics scratch, so a chunk's launch starts on the SMs its predecessor's tail frees.
-    if (nchunk > 1) {
-        if (!c->st_c2) CK(cudaStreamCreateWithFlags(&c->st_c2, cudaStreamNonBlocking));
-        if (c->scratch2_bytes < sbytes) {
-            if (c->scratch2) cudaFree(c->scratch2);
-            c->scratch2 = nullptr;
-            c->scratch2_bytes = 0;
-            CK(cudaMalloc((void **)&c->scratch2, sbytes));
-            c->scratch2_bytes = sbytes;
-        }
-        if (!c->partials2) CK(cudaMalloc(&c->partials2, reduce_partials_bytes()));
-    }
     while ((int)c->pipe_ev.size() < 2 * nchunk) {
         cudaEvent_t e;
         CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -819,15 +800,13 @@ int radm2_rosenbrock_host(radm2_ctx *c, int ncell, double *VAR, const double *FI
         if (RC_N2O5) CK(cudaMemcpyAsync(c->rcn + lo, sr + l, sizeof(double) * m, cudaMemcpyDeviceToDevice, c->st_up));
         CK(launch_aos_to_soa(m, NPH, c->ld, sj + l * NPH, c->jv + lo, c->st_up));
         CK(cudaEventRecord(c->pipe_ev[2 * k], c->st_up));
-        // integrate the chunk (even chunks on the context's stream, odd ones on the second)
-        cudaStream_t cs = (k & 1) ? c->st_c2 : c->st;
-        CK(cudaStreamWaitEvent(cs, c->pipe_ev[2 * k], 0));
+        // integrate the chunk
+        CK(cudaStreamWaitEvent(c->st, c->pipe_ev[2 * k], 0));
         CK(launch_rconst(m, c->ld, c->jv + lo, c->temp + lo, c->fix + lo, RC_N2O5 ? c->rcn + lo : nullptr,
-                         c->rconst + lo, cs));
-        if (c->mlp) CK(mlp_enqueue_seed(c, c->mlp, dt, 0, lo, m, cs));
-        CK(cudaMemsetAsync(c->queue + k, 0, sizeof(int), cs));
+                         c->rconst + lo, c->st));
+        if (c->mlp) CK(mlp_enqueue_seed(c, c->mlp, dt, 0, lo, m));
+        CK(cudaMemsetAsync(c->queue + k, 0, sizeof(int), c->st));
         SolveArgs a = make_args(c, p, c->queue + k);
-        if (k & 1) a.scratch = c->scratch2;
         a.ncell = m;
         a.var += lo;
         a.fix += lo;
@@ -844,10 +823,10 @@ int radm2_rosenbrock_host(radm2_ctx *c, int ncell, double *VAR, const double *FI
         if (c->o.schedule == RADM2_SCHED_COOP) kg = std::min(grid, (m + 31) / 32);
         else if (c->o.schedule == RADM2_SCHED_PERSISTENT) kg = std::min(grid, (m + cpb - 1) / cpb);
         else kg = (m + cpb - 1) / cpb;
-        CK(launch_solver(c, a, bs, std::max(kg, 1), cs));
-        CK(launch_reduce(m, c->status + lo, c->nacc + lo, c->nrej + lo, c->texit + lo, c->hexit + lo,
-                         (k & 1) ? c->partials2 : c->partials, c->d_res + k, cs));
-        CK(cudaEventRecord(c->pipe_ev[2 * k + 1], cs));
+        CK(launch_solver(c, a, bs, std::max(kg, 1)));
+        CK(launch_reduce(m, c->status + lo, c->nacc + lo, c->nrej + lo, c->texit + lo, c->hexit + lo, c->partials,
+                         c->d_res + k, c->st));
+        CK(cudaEventRecord(c->pipe_ev[2 * k + 1], c->st));
         // down: this chunk's states
         CK(cudaStreamWaitEvent(c->st_down, c->pipe_ev[2 * k + 1], 0));
         CK(launch_soa_to_aos(m, NVAR, c->ld, c->var + lo, so + l * NVAR, c->st_down));
@@ -855,10 +834,6 @@ int radm2_rosenbrock_host(radm2_ctx *c, int ncell, double *VAR, const double *FI
                            c->st_down));
     }
     c->use_order = order_was;
-    if (nchunk > 1) {  // the odd chunks' statistics are ready before the read-back on the context's stream
-        const int ko = ((nchunk - 1) & 1) ? nchunk - 1 : nchunk - 2;  // last odd chunk
-        CK(cudaStreamWaitEvent(c->st, c->pipe_ev[2 * ko + 1], 0));
-    }
     CK(cudaMemcpyAsync(c->h_res, c->d_res, sizeof(RunResult) * nchunk, cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
     CK(cudaStreamSynchronize(c->st_down));
@@ -1294,7 +1269,7 @@ int radm2_autotune(radm2_ctx *c, double dt, const double *AbsTol, const double *
 size_t radm2_device_bytes(const radm2_ctx *c)
 {
     if (!c) return 0;
-    return c->bytes + c->scratch_bytes + c->scratch2_bytes + c->stage_bytes;
+    return c->bytes + c->scratch_bytes + c->stage_bytes;
 }
 
 int radm2_coop_selftest_wait_limit(radm2_ctx *c)

@@ -13,10 +13,6 @@ struct radm2_ctx {
     cudaStream_t own = nullptr;
     cudaStream_t st = nullptr;
     cudaStream_t st_up = nullptr, st_down = nullptr;  // copy streams of the pipelined host path
-    cudaStream_t st_c2 = nullptr;                      // its second compute stream (odd chunks)
-    double *scratch2 = nullptr;                        // solver scratch of the second compute stream
-    size_t scratch2_bytes = 0;
-    void *partials2 = nullptr;                         // statistics scratch of the second compute stream
     std::vector<cudaEvent_t> pipe_ev;                 // per chunk: inputs up, chunk integrated
     int ncell = 0, ld = 0;
     double *var = nullptr, *fix = nullptr, *temp = nullptr, *rcn = nullptr, *jv = nullptr, *rconst = nullptr;
@@ -66,9 +62,7 @@ namespace radm2 {
 void ctx_drop_graph(radm2_ctx *c);
 // Learned seeding (radm2_mlp.cu): buffers, then the stream-ordered kernels.
 int mlp_prepare_seed(radm2_ctx *c, radm2_mlp *m, int order);
-// stream: nullptr = the context's stream
-cudaError_t mlp_enqueue_seed(radm2_ctx *c, radm2_mlp *m, double dt, int order, int lo = 0, int count = -1,
-                             cudaStream_t stream = nullptr);
+cudaError_t mlp_enqueue_seed(radm2_ctx *c, radm2_mlp *m, double dt, int order, int lo = 0, int count = -1);
 unsigned int mlp_generation(const radm2_mlp *m);
 void mlp_detach(radm2_mlp *m);
 }  // namespace radm2

@@ -912,24 +912,20 @@ void radm2::mlp_detach(radm2_mlp *m) { m->attached--; }
 
 // Stream-ordered seeding on the context's stream (capturable): features -> network ->
 // per-cell h0 (and the descending-cost order when asked).
-cudaError_t radm2::mlp_enqueue_seed(radm2_ctx *c, radm2_mlp *m, double dt, int order, int lo, int count,
-                                    cudaStream_t stream)
+cudaError_t radm2::mlp_enqueue_seed(radm2_ctx *c, radm2_mlp *m, double dt, int order, int lo, int count)
 {
-    // cells [lo, lo + count) (count < 0: all); a sub-range gets h0 only, no order, and uses the
-    // rows of the work arrays at its own cells, so sub-ranges on different streams do not meet
+    // cells [lo, lo + count) (count < 0: all); a sub-range gets h0 only, no order
     const int n = count < 0 ? c->ncell : count;
-    const size_t off = count < 0 ? 0 : (size_t)lo;
     if (count >= 0) order = 0;
-    cudaStream_t st = stream ? stream : c->st;
-    float *sx = c->seed_x + off * NFEAT, *sy = c->seed_y + off * NY;
     (void)cudaGetLastError();
-    k_features<<<(n + FEAT_BLOCK - 1) / FEAT_BLOCK, FEAT_BLOCK, 0, st>>>(n, c->ld, c->var + lo, c->fix + lo,
-                                                                      c->temp + lo, c->jv + lo, (float)dt, sx);
+    k_features<<<(n + FEAT_BLOCK - 1) / FEAT_BLOCK, FEAT_BLOCK, 0, c->st>>>(n, c->ld, c->var + lo, c->fix + lo,
+                                                                         c->temp + lo, c->jv + lo, (float)dt,
+                                                                         c->seed_x);
     cudaError_t e = cudaGetLastError();
-    if (e == cudaSuccess) e = forward(m, n, sx, sy, false, st);
+    if (e == cudaSuccess) e = forward(m, n, c->seed_x, c->seed_y, false, c->st);
     if (e == cudaSuccess) {
-        k_seed<<<(n + 127) / 128, 128, 0, st>>>(n, sy, m->ymean[0], m->ystd[0], m->ymean[1], m->ystd[1], m->h0_scale,
-                                                c->h0 + lo, c->seed_keys + off, c->seed_idx + off);
+        k_seed<<<(n + 127) / 128, 128, 0, c->st>>>(n, c->seed_y, m->ymean[0], m->ystd[0], m->ymean[1], m->ystd[1],
+                                                   m->h0_scale, c->h0 + lo, c->seed_keys, c->seed_idx);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess && order == 1) {
