@@ -33,12 +33,24 @@
 //   RADM2_COOP_RECIP   1 = reciprocal pivots (the fast form), 0 = the reference's divisions
 //                      (that file is compiled without multiply-add contraction)
 //   RADM2_COOP_KERNEL  the kernel's name
+//   RADM2_COOP_TABLES  0 (default): the unrolled per-role LU and solve code; 1: the LU and
+//                      the triangular solves run from per-role operation tables
+//                      (gen/radm2_coop_g<G>_ops.h) through a small interpreter.  The
+//                      tables end the instruction-fetch stalls but execute 2.4x the
+//                      instructions; measured 27% slower on B200, so not the default.
 #pragma once
 
 #include "radm2_device.cuh"
 
+#ifndef RADM2_COOP_TABLES
+#define RADM2_COOP_TABLES 0
+#endif
+
 #if RADM2_COOP_G == 4
 #include "gen/radm2_coop_g4.h"
+#if RADM2_COOP_TABLES
+#include "gen/radm2_coop_g4_ops.h"
+#endif
 #define RADM2_COOP_NS RADM2_COOP_G4_NS
 #define RADM2_COOP_OWN_INC "gen/radm2_coop_g4_own.inc"
 #define RADM2_COOP_FUN_INC "gen/radm2_coop_g4_fun.inc"
@@ -53,6 +65,9 @@
 #endif
 #elif RADM2_COOP_G == 8
 #include "gen/radm2_coop_g8.h"
+#if RADM2_COOP_TABLES
+#include "gen/radm2_coop_g8_ops.h"
+#endif
 #define RADM2_COOP_NS RADM2_COOP_G8_NS
 #define RADM2_COOP_OWN_INC "gen/radm2_coop_g8_own.inc"
 #define RADM2_COOP_FUN_INC "gen/radm2_coop_g8_fun.inc"
@@ -149,6 +164,136 @@ static __device__ __noinline__ void coop_fun(int role, const double *vb, const d
 #undef RC
 #undef COOP_ROLE
 }
+
+#if RADM2_COOP_TABLES
+// ---- table-driven LU and triangular solves
+// Every role runs the same few loops over its own operation words, so the instruction cache
+// holds one small interpreter instead of every role's unrolled rows.  A word is
+// opcode << 28 | A << 18 | B << 8 | C; the streams (mech/emit_coop.py) keep each slot's
+// operations in the order of the unrolled row blocks, so results are the same.
+enum : unsigned {
+    COOP_OP_END = 0, COOP_OP_CHECK = 1, COOP_OP_WAIT = 2, COOP_OP_PIVOT = 3, COOP_OP_UPD = 4, COOP_OP_RCP = 5,
+    COOP_OP_DONE = 6, COOP_OP_ROW = 7, COOP_OP_TERM = 8, COOP_OP_STORE = 9, COOP_OP_STORE_DIAG = 10
+};
+#define COOP_FA(w) (((w) >> 18) & 1023u)
+#define COOP_FB(w) (((w) >> 8) & 1023u)
+#define COOP_FC(w) ((w)&255u)
+
+// LU: CHECK(diag) records a zero pivot; WAIT(row) waits for another role's finished row;
+// PIVOT(slot i,j; diag j; n) forms the multiplier and is followed by n UPD(slot i,k; slot
+// j,k) updates, four at a time (distinct targets, sources in the pivot row); RCP(diag) stores
+// the reciprocal pivot; DONE(row) publishes the row.
+static __device__ __forceinline__ int coop_lu_run(const unsigned *p, double *lu, int lane, volatile int *flags,
+                                                 int seq, int werr, int *sing)
+{
+    double *const L = lu + lane;  // slot s of this lane's cell at L[s * 32]
+    for (;;) {
+        const unsigned w = __ldg(p);
+        const unsigned op = w >> 28;
+        if (op == COOP_OP_PIVOT) {
+            const unsigned n = COOP_FC(w);
+#if RADM2_COOP_RECIP
+            const double a = -L[COOP_FA(w) * 32] * L[COOP_FB(w) * 32];
+#else
+            const double a = -L[COOP_FA(w) * 32] / L[COOP_FB(w) * 32];
+#endif
+            L[COOP_FA(w) * 32] = -a;
+            p++;
+            unsigned q = 0;
+            for (; q + 4 <= n; q += 4, p += 4) {
+                const unsigned w0 = __ldg(p), w1 = __ldg(p + 1), w2 = __ldg(p + 2), w3 = __ldg(p + 3);
+                const double u0 = L[COOP_FB(w0) * 32], u1 = L[COOP_FB(w1) * 32], u2 = L[COOP_FB(w2) * 32],
+                             u3 = L[COOP_FB(w3) * 32];
+                const double v0 = L[COOP_FA(w0) * 32], v1 = L[COOP_FA(w1) * 32], v2 = L[COOP_FA(w2) * 32],
+                             v3 = L[COOP_FA(w3) * 32];
+                L[COOP_FA(w0) * 32] = v0 + a * u0;
+                L[COOP_FA(w1) * 32] = v1 + a * u1;
+                L[COOP_FA(w2) * 32] = v2 + a * u2;
+                L[COOP_FA(w3) * 32] = v3 + a * u3;
+            }
+            for (; q < n; q++, p++) {
+                const unsigned w0 = __ldg(p);
+                L[COOP_FA(w0) * 32] = L[COOP_FA(w0) * 32] + a * L[COOP_FB(w0) * 32];
+            }
+            continue;
+        }
+        p++;
+        if (op == COOP_OP_END) break;
+        if (op == COOP_OP_CHECK) {
+            if (L[COOP_FA(w) * 32] == 0.0) sing[lane] = 1;
+        } else if (op == COOP_OP_WAIT) {
+            if (!werr) werr = coop_wait(flags + COOP_FC(w), seq, COOP_WAIT_CYCLES);
+        } else if (op == COOP_OP_RCP) {
+            L[COOP_FA(w) * 32] = 1.0 / L[COOP_FA(w) * 32];
+        } else if (op == COOP_OP_DONE) {
+            coop_signal(flags + COOP_FC(w), seq);
+        }
+    }
+    return werr;
+}
+
+// Triangular solve rows: ROW(k; n) starts x_k's sum, n TERM(slot; j) subtract G(slot) x_j in
+// the row's order, STORE(k) or STORE_DIAG(k; diag) ends it (the backward rows times the
+// reciprocal pivot, or divided by the pivot); WAIT and DONE as for the LU.
+static __device__ __forceinline__ int coop_solve_run(const unsigned *p, const double *lu, double *xs, int lane,
+                                                    volatile int *flags, int seq, int werr)
+{
+    const double *const L = lu + lane;
+    double *const X = xs + lane;
+    for (;;) {
+        const unsigned w = __ldg(p++);
+        const unsigned op = w >> 28;
+        if (op == COOP_OP_ROW) {
+            const unsigned n = COOP_FC(w);
+            double acc = X[COOP_FA(w) * 32];
+            unsigned q = 0;
+            for (; q + 4 <= n; q += 4, p += 4) {
+                const unsigned w0 = __ldg(p), w1 = __ldg(p + 1), w2 = __ldg(p + 2), w3 = __ldg(p + 3);
+                const double g0 = L[COOP_FA(w0) * 32], g1 = L[COOP_FA(w1) * 32], g2 = L[COOP_FA(w2) * 32],
+                             g3 = L[COOP_FA(w3) * 32];
+                const double x0 = X[COOP_FB(w0) * 32], x1 = X[COOP_FB(w1) * 32], x2 = X[COOP_FB(w2) * 32],
+                             x3 = X[COOP_FB(w3) * 32];
+                acc = acc - g0 * x0;
+                acc = acc - g1 * x1;
+                acc = acc - g2 * x2;
+                acc = acc - g3 * x3;
+            }
+            for (; q < n; q++, p++) {
+                const unsigned w0 = __ldg(p);
+                acc = acc - L[COOP_FA(w0) * 32] * X[COOP_FB(w0) * 32];
+            }
+            const unsigned we = __ldg(p++);
+            if ((we >> 28) == COOP_OP_STORE) {
+                X[COOP_FA(we) * 32] = acc;
+            } else {
+#if RADM2_COOP_RECIP
+                X[COOP_FA(we) * 32] = acc * L[COOP_FB(we) * 32];
+#else
+                X[COOP_FA(we) * 32] = acc / L[COOP_FB(we) * 32];
+#endif
+            }
+        } else if (op == COOP_OP_END) {
+            break;
+        } else if (op == COOP_OP_WAIT) {
+            if (!werr) werr = coop_wait(flags + COOP_FC(w), seq, COOP_WAIT_CYCLES);
+        } else if (op == COOP_OP_DONE) {
+            coop_signal(flags + COOP_FC(w), seq);
+        }
+    }
+    return werr;
+}
+#if RADM2_COOP_RECIP
+#define COOP_LU_OPS coop_lu_ops
+#define COOP_LU_START coop_lu_start
+#define COOP_BWD_OPS coop_bwd_ops
+#define COOP_BWD_START coop_bwd_start
+#else
+#define COOP_LU_OPS coop_lu_div_ops
+#define COOP_LU_START coop_lu_div_start
+#define COOP_BWD_OPS coop_bwd_div_ops
+#define COOP_BWD_START coop_bwd_div_start
+#endif
+#endif
 
 __global__ void __launch_bounds__(32 * RADM2_COOP_G, 1) RADM2_COOP_KERNEL(const SolveArgs a)
 {
@@ -303,6 +448,10 @@ __global__ void __launch_bounds__(32 * RADM2_COOP_G, 1) RADM2_COOP_KERNEL(const 
         lu_seq++;
         if (a.coop_selftest && role == 1)  // a flag nothing sets: the bounded wait runs out
             COOP_WAIT_ON(vflag + COOP_FLAG_NEVER, lu_seq, COOP_SELFTEST_WAIT_CYCLES);
+#if RADM2_COOP_TABLES
+        werr = coop_lu_run(COOP_LU_OPS + __ldg(COOP_LU_START + role), lu, lane, vflag + COOP_FLAG_LU, lu_seq, werr,
+                           ism + COOP_SING);
+#else
         {
 #define G(s) SW(lu, s)
 #define LU_T double
@@ -317,6 +466,7 @@ __global__ void __launch_bounds__(32 * RADM2_COOP_G, 1) RADM2_COOP_KERNEL(const 
 #undef LU_T
 #undef G
         }
+#endif
         __syncthreads();
         if (active && ism[COOP_SING + lane]) {
             status = -8;
@@ -367,10 +517,20 @@ __global__ void __launch_bounds__(32 * RADM2_COOP_G, 1) RADM2_COOP_KERNEL(const 
 #define SOLVE_WAIT(j) COOP_WAIT_ON(vflag + COOP_FLAG_SV + (j), sv_seq, COOP_WAIT_CYCLES)
 #define SOLVE_DONE(i) coop_signal(vflag + COOP_FLAG_SV + (i), sv_seq)
             sv_seq++;
+#if RADM2_COOP_TABLES
+            werr = coop_solve_run(coop_fwd_ops + __ldg(coop_fwd_start + role), lu, xs, lane, vflag + COOP_FLAG_SV,
+                                  sv_seq, werr);
+#else
 #include RADM2_COOP_FWD_INC
+#endif
             __syncthreads();
             sv_seq++;
+#if RADM2_COOP_TABLES
+            werr = coop_solve_run(COOP_BWD_OPS + __ldg(COOP_BWD_START + role), lu, xs, lane, vflag + COOP_FLAG_SV,
+                                  sv_seq, werr);
+#else
 #include RADM2_COOP_BWD_INC
+#endif
             __syncthreads();
 #undef SOLVE_WAIT
 #undef SOLVE_DONE

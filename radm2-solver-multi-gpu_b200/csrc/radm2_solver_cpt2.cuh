@@ -138,6 +138,16 @@ __global__ void __launch_bounds__(BS, 1) k_rosenbrock_cpt2(const SolveArgs a)
             }
             ghinv[v] = 1.0 / (dir * H[v] * RADM2_ROS_GAMMA0);
         }
+#if RADM2_JACLU
+#pragma unroll
+        for (int v = 0; v < 2; v++)
+            if (go[v] && ph_jaclu<VB, double>(rcy(v) + RCY_Y * VB, rcy(v) + RCY_RC * VB, lu(v), fix0[v], fix1[v],
+                                              ghinv[v])) {
+                status[v] = -8;
+                done[v] = true;
+                go[v] = false;
+            }
+#else
 #pragma unroll
         for (int v = 0; v < 2; v++)
             if (go[v]) ph_jac<VB, double>(rcy(v) + RCY_Y * VB, rcy(v) + RCY_RC * VB, lu(v), fix0[v], fix1[v], ghinv[v]);
@@ -148,6 +158,7 @@ __global__ void __launch_bounds__(BS, 1) k_rosenbrock_cpt2(const SolveArgs a)
                 done[v] = true;
                 go[v] = false;
             }
+#endif
 #pragma unroll 1
         for (int stage = 0; stage < 3; stage++) {
 #pragma unroll

@@ -379,6 +379,7 @@ def emit_cuda(m, out_dir):
         fd, fs = emit_lu(crow, diag, icol, nvar, out_dir, recip)
         if not recip:
             flops["decomp"], flops["solve"] = fd, fs
+        emit_jaclu(m, crow, diag, icol, nvar, out_dir, recip)
 
     h.append("\n/* Algorithmic flop counts per call, counted from the emitted expressions */\n")
     for k, v in sorted(flops.items()):
@@ -459,6 +460,109 @@ def emit_lu(crow, diag, icol, nvar, out_dir, recip):
         f += 1
     write(os.path.join(out_dir, "radm2_solve%s.inc" % sfx), body)
     return fdec, f
+
+
+def slot_chain(t):
+    """A Jacobian slot's expression as its left-to-right chain [(None, t0), (op, t1), ...]."""
+    chain = []
+    node = t
+    while node[0] == "bin" and node[1] in "+-":
+        chain.append((node[1], node[3]))
+        node = node[2]
+    chain.append((None, node))
+    chain.reverse()
+    return chain
+
+
+def term_b(term):
+    """The one partial B_b a Jacobian term multiplies."""
+    bs = []
+
+    def walkb(x):
+        if x[0] == "ref" and x[1] == "B":
+            bs.append(x[2])
+        elif x[0] == "bin":
+            walkb(x[2]); walkb(x[3])
+        elif x[0] == "neg":
+            walkb(x[1])
+    walkb(term)
+    assert len(bs) == 1, term
+    return bs[0]
+
+
+def count_loads(t):
+    """Array reads (RC, V) in an expression."""
+    if t[0] == "ref":
+        return 1 if t[1] in ("RCT", "V") else 0
+    if t[0] == "bin":
+        return count_loads(t[2]) + count_loads(t[3])
+    if t[0] == "neg":
+        return count_loads(t[1])
+    if t[0] == "call":
+        return sum(count_loads(a) for a in t[2])
+    return 0
+
+
+def emit_jaclu(m, crow, diag, icol, nvar, out_dir, recip):
+    """Jacobian and LU fused row by row: row k's slots of G = -J + ghinv I are formed in
+    registers (each slot the same left-to-right sum of its partials as the partial-major
+    Jacobian, so the same value), its pivot is checked, the row is eliminated against the
+    finished rows above it exactly as emit_lu does, and only then stored.  The matrix is
+    written once per factorisation instead of written by the Jacobian and read back by
+    the LU; the price is that a partial feeding several rows is formed once per row."""
+    sfx = "_rcp" if recip else ""
+    r = Renderer(kernel_ref, kernel_var)
+    dset = set(diag)
+    body = [BANNER, "/* Jacobian (mgpu.cu:1685-2652) and pivot-free LU (mgpu.cu:2746-2779) fused row by\n"
+            " * row.  Inputs: RC(r), V(i), FIX(k).  Accessors: G(s), LU_T; JAC_VAL(e),\n"
+            " * JAC_VAL_DIAG(e) and JAC_VAL_ZERO(is_diag) turn a Jacobian slot into a slot of G;\n"
+            " * LU_PIVOT_CHECK(row, diag_value); LU_STEP_FENCE bounds the loads in flight.%s */\n"
+            % ("\n * Reciprocal form: the diagonal slots hold 1/U(k,k) on exit." if recip else ""),
+            "#ifndef LU_STEP_FENCE\n#define LU_STEP_FENCE do { } while (0)\n#endif\n"]
+    since_fence = 0
+    for k in range(nvar):
+        body.append("{ /* row %d */\n" % k)
+        for sl in range(crow[k], crow[k + 1]):
+            t = m["jvs"][sl]
+            c = icol[sl]
+            if is_zero(t):
+                body.append("  LU_T w%d = JAC_VAL_ZERO(%d);\n" % (c, 1 if sl in dset else 0))
+                continue
+            chain = slot_chain(t)
+            defs = []
+            expr = None
+            for pos, (op, term) in enumerate(chain):
+                b = term_b(term)
+                bt = m["bvals"][str(b)]
+                defs.append("const double b%d = %s;" % (b, r(bt)))
+                since_fence += count_loads(bt)
+                expr = r(term) if pos == 0 else "(%s %s %s)" % (expr, op, r(term))
+            body.append("  LU_T w%d;\n  { %s\n    w%d = %s(%s); }\n"
+                        % (c, "\n    ".join(defs), c, "JAC_VAL_DIAG" if sl in dset else "JAC_VAL", expr))
+            if since_fence >= LU_FENCE_LOADS:
+                body.append("  LU_STEP_FENCE;\n")
+                since_fence = 0
+        body.append("  LU_PIVOT_CHECK(%d, w%d);\n" % (k, k))
+        for kk in range(crow[k], diag[k]):
+            j = icol[kk]
+            if recip:
+                body.append("  { const LU_T a = -w%d * G(%d); w%d = -a;\n" % (j, diag[j], j))
+            else:
+                body.append("  { const LU_T a = -w%d / G(%d); w%d = -a;\n" % (j, diag[j], j))
+            for jj in range(diag[j] + 1, crow[j + 1]):
+                body.append("    w%d += a * G(%d);\n" % (icol[jj], jj))
+            since_fence += crow[j + 1] - diag[j]
+            if since_fence >= LU_FENCE_LOADS:
+                body.append("  LU_STEP_FENCE;\n")
+                since_fence = 0
+            body.append("  }\n")
+        for sl in range(crow[k], crow[k + 1]):
+            if recip and sl == diag[k]:
+                body.append("  G(%d) = (LU_T)1 / w%d;\n" % (sl, icol[sl]))
+            else:
+                body.append("  G(%d) = w%d;\n" % (sl, icol[sl]))
+        body.append("}\n")
+    write(os.path.join(out_dir, "radm2_jaclu%s.inc" % sfx), body)
 
 
 # ----------------------------------------------------------------------------- oracle C

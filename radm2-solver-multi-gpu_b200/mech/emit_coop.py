@@ -151,6 +151,103 @@ def schedule_solve(crow, diag, icol, nvar, nroles):
     return own_l, own_u, span_l, span_u
 
 
+# ---- operation streams for the table-driven LU and solves
+# One 32-bit word per operation: opcode (4 bits) | A (10 bits) | B (10 bits) | C (8 bits).
+OPS = {"END": 0, "CHECK": 1, "WAIT": 2, "PIVOT": 3, "UPD": 4, "RCP": 5, "DONE": 6, "ROW": 7, "TERM": 8,
+       "STORE": 9, "STORE_DIAG": 10}
+
+
+def op_word(op, a=0, b=0, c=0):
+    assert 0 <= a < 1024 and 0 <= b < 1024 and 0 <= c < 256, (op, a, b, c)
+    return (OPS[op] << 28) | (a << 18) | (b << 8) | c
+
+
+def lu_op_streams(crow, diag, icol, nvar, owner, recip):
+    """Per role, the LU of its rows as operation words: CHECK(diag) at a row's start,
+    WAIT(row) before the first pivot on a row another role owns, PIVOT(slot i,j; diag j;
+    n) followed by n UPD(slot i,k; slot j,k), RCP(diag) (reciprocal form), DONE(row).  The
+    same operations in the same order per slot as the unrolled row blocks."""
+    nroles = max(owner) + 1
+    streams = [[] for _ in range(nroles)]
+    for ro in range(nroles):
+        waited = set()
+        out = streams[ro]
+        for i in range(nvar):
+            if owner[i] != ro:
+                continue
+            out.append(op_word("CHECK", diag[i]))
+            col_slot = {icol[sl]: sl for sl in range(crow[i], crow[i + 1])}
+            for kk in range(crow[i], diag[i]):
+                j = icol[kk]
+                if owner[j] != ro and j not in waited:
+                    if recip or crow[j] != diag[j]:
+                        out.append(op_word("WAIT", c=j))
+                    waited.add(j)
+                ups = list(range(diag[j] + 1, crow[j + 1]))
+                out.append(op_word("PIVOT", kk, diag[j], len(ups)))
+                for jj in ups:
+                    out.append(op_word("UPD", col_slot[icol[jj]], jj))
+            if recip:
+                out.append(op_word("RCP", diag[i]))
+            out.append(op_word("DONE", c=i))
+        out.append(op_word("END"))
+    return streams
+
+
+def solve_op_streams(crow, diag, icol, nvar, own_l, own_u, recip):
+    """Per role, the forward rows (ROW(k, n), n TERM(slot, j), STORE(k), DONE(k)) and, as a
+    separate stream, the backward rows (... STORE_DIAG(k, diag k) ...), with WAIT(row) before
+    another role's row is read.  Each row's terms in the unrolled order."""
+    nroles = max(o for o in own_u if o is not None) + 1
+    fwd = [[] for _ in range(nroles)]
+    bwd = [[] for _ in range(nroles)]
+    lo = [[s for s in range(crow[i], diag[i])] for i in range(nvar)]
+    for ro in range(nroles):
+        waited = set()
+        out = fwd[ro]
+        for k in range(nvar):
+            if own_l[k] != ro:
+                continue
+            for s in lo[k]:
+                j = icol[s]
+                if lo[j] and own_l[j] != ro and j not in waited:
+                    out.append(op_word("WAIT", c=j))
+                    waited.add(j)
+            out.append(op_word("ROW", k, 0, len(lo[k])))
+            for s in lo[k]:
+                out.append(op_word("TERM", s, icol[s]))
+            out.append(op_word("STORE", k))
+            out.append(op_word("DONE", c=k))
+        out.append(op_word("END"))
+        waited = set()
+        out = bwd[ro]
+        for k in reversed(range(nvar)):
+            if own_u[k] != ro:
+                continue
+            ups = list(range(diag[k] + 1, crow[k + 1]))
+            for s in ups:
+                j = icol[s]
+                if own_u[j] != ro and j not in waited:
+                    out.append(op_word("WAIT", c=j))
+                    waited.add(j)
+            out.append(op_word("ROW", k, 0, len(ups)))
+            for s in ups:
+                out.append(op_word("TERM", s, icol[s]))
+            out.append(op_word("STORE_DIAG", k, diag[k]))
+            out.append(op_word("DONE", c=k))
+        out.append(op_word("END"))
+    return fwd, bwd
+
+
+def flat(streams):
+    """Concatenated words and the start of every role's stream."""
+    words, starts = [], []
+    for st in streams:
+        starts.append(len(words))
+        words.extend(st)
+    return words, starts
+
+
 def kref(arr, i):
     return {"RCT": "RC(%d)", "V": "V(%d)", "F": "FIX(%d)", "A": "a%d", "B": "b%d"}[arr] % i
 
@@ -360,6 +457,29 @@ def emit_role_code(m, G, out_dir):
             body.append("} break;\n")
         body.append("default: break;\n}\n")
         emit.write(os.path.join(out_dir, "radm2_coop_g%d_bwd%s.inc" % (G, sfx)), body)
+
+    # ---- operation streams of the table-driven LU and solves
+    tabs = []
+    for name, streams in (("lu", lu_op_streams(crow, diag, icol, nvar, lu_owner, True)),
+                          ("lu_div", lu_op_streams(crow, diag, icol, nvar, lu_owner, False))):
+        w, st = flat(streams)
+        tabs.append((name, w, st))
+    for recip in (True, False):
+        fwd, bwd = solve_op_streams(crow, diag, icol, nvar, own_l, own_u, recip)
+        if recip:
+            w, st = flat(fwd)
+            tabs.append(("fwd", w, st))
+        w, st = flat(bwd)
+        tabs.append(("bwd" if recip else "bwd_div", w, st))
+    body = [banner, "/* Operation streams of the table-driven LU and triangular solves, %d roles: per\n"
+            " * stream, the words of every role back to back and each role's first word.  Word:\n"
+            " * opcode << 28 | A << 18 | B << 8 | C (see radm2_coop.cuh). */\n" % G]
+    for name, w, st in tabs:
+        body.append("static __device__ const unsigned coop_%s_ops[%d] = {%s};\n" % (
+            name, len(w), ",".join("0x%08xu" % x for x in w)))
+        body.append("static __device__ const int coop_%s_start[%d] = {%s};\n" % (name, len(st), ",".join(map(str, st))))
+    emit.write(os.path.join(out_dir, "radm2_coop_g%d_ops.h" % G), body)
+    notes.append("operation words: " + ", ".join("%s %d" % (n, len(w)) for n, w, _ in tabs))
 
     h = [banner, "#pragma once\n/* Cooperative kernel with %d roles: %s. */\n" % (G, "; ".join(notes)),
          "#define RADM2_COOP_G%d_NS %d  /* most species owned by one role */\n" % (G, ns)]
