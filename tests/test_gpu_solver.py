@@ -287,6 +287,30 @@ def test_pipelined_host_integration_matches_separate_calls(nchunk):
     assert rpar[10] == rpar0[10] and rpar[11] == rpar0[11]
 
 
+@pytest.mark.parametrize("threads", [32, 256])
+def test_pipelined_host_many_chunks(threads):
+    """Many small chunks of stiff mixed cells (48 launches, each with its own queue counter,
+    copies and transposes in flight on the copy streams): states and counters equal one
+    whole-batch call bit for bit, and a second call on the same context gives the same
+    again."""
+    cells = inputs.make_cells(100000, 12, "mixed")
+    atol, rtol = np.ones(59), np.full(59, 1e-3)
+    opts = dict(schedule=radm2b200.SCHED_PERSISTENT, block_threads=threads)
+    with radm2b200.Solver(**opts) as s:
+        s.set_cells(cells)
+        ipar0, rpar0 = radm2b200.default_params(hstart=6.0)
+        assert s.rosenbrock(0.0, 600.0, atol, rtol, rpar0, ipar0) == 1
+        y0 = s.get_state()
+    with radm2b200.Solver(**opts) as s:
+        for _ in range(2):
+            y = np.ascontiguousarray(cells["VAR"]).copy()
+            ipar, rpar = radm2b200.default_params(hstart=6.0)
+            assert s.rosenbrock_host(y, cells["FIX"], cells["TEMP"], cells["RC_N2O5"], cells["JV"], 0.0, 600.0,
+                                     atol, rtol, rpar, ipar, nchunk=48) == 1
+            assert np.array_equal(y, y0)
+            assert list(ipar[10:17]) == list(ipar0[10:17])
+
+
 def test_pipelined_host_integration_with_seeding():
     from radm2b200 import seeding
     cells = inputs.make_cells(12000, 10, "mixed")
