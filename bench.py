@@ -69,6 +69,8 @@ WORKLOADS = {
 }
 ATOL, RTOL, RTOL_TIGHT = 1.0, 1.0e-3, 1.0e-8
 SCHED_NAMES = {0: "static", 1: "persistent", 2: "coop"}
+# --placement names -> RADM2_PLACE_* (include/radm2.h)
+PLACEMENTS = {"": 0, "global": 0, "lu-smem": 1, "all-smem": 3, "lu-tmem": 4}
 
 
 # HBM copy bandwidth of a B200 when no measured peak file is present (GB/s).
@@ -91,6 +93,8 @@ def parse():
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shape")
     ap.add_argument("--block-threads", type=int, default=0)
     ap.add_argument("--blocks-per-sm", type=int, default=0)
+    ap.add_argument("--placement", default="", choices=["", "global", "lu-smem", "all-smem", "lu-tmem"],
+                    help="working-set placement (sets the launch shape by hand: no autotuning)")
     ap.add_argument("--accuracy-cells", type=int, default=8192)
     ap.add_argument("--weights", default="", help="seeding network stored by --save-weights (skip training)")
     ap.add_argument("--save-weights", default="")
@@ -408,8 +412,8 @@ def main():
     # ---- headline arm: inputs resident in HBM, K splits as one CUDA graph
     solver = radm2b200.Solver(precision=prec, schedule=sched, refine_sweeps=refine, device=local,
                               block_threads=args.block_threads, blocks_per_sm=args.blocks_per_sm,
-                              parity=1 if args.parity else 0)
-    tune = not args.no_autotune and not args.block_threads and not args.blocks_per_sm
+                              parity=1 if args.parity else 0, placement=PLACEMENTS[args.placement])
+    tune = not args.no_autotune and not args.block_threads and not args.blocks_per_sm and not args.placement
     main_arm = timed_arm(solver, learned, tune=tune)
     value = ncell * world * args.steps / (main_arm["el_ms"] * 1e-3)
     y_main = solver.get_state() if rank == 0 else None

@@ -270,7 +270,7 @@ cudaError_t variant_info(radm2_ctx *c, int bs, SolverInfo *info)
 int default_block_threads(const radm2_opts &o)
 {
     if (o.schedule == RADM2_SCHED_COOP) return 256;
-    if (o.placement == RADM2_PLACE_GLOBAL) return 128;
+    if (o.placement == RADM2_PLACE_GLOBAL || o.placement == RADM2_PLACE_LU_TMEM) return 128;
     if (o.placement == RADM2_PLACE_LU_SMEM && o.precision == RADM2_PREC_FP32LU) return 64;
     return 32;
 }
@@ -495,8 +495,10 @@ int radm2_create(radm2_ctx **out, const radm2_opts *opts)
         (o.precision != RADM2_PREC_FP64 || o.placement != RADM2_PLACE_GLOBAL || o.min_blocks > 1))
         return RADM2_E_ARG;
     if (o.refine_sweeps < 0 || o.refine_sweeps > 2) return RADM2_E_ARG;
-    if (o.placement != RADM2_PLACE_GLOBAL && o.placement != RADM2_PLACE_LU_SMEM && o.placement != RADM2_PLACE_ALL_SMEM)
+    if (o.placement != RADM2_PLACE_GLOBAL && o.placement != RADM2_PLACE_LU_SMEM && o.placement != RADM2_PLACE_ALL_SMEM &&
+        o.placement != RADM2_PLACE_LU_TMEM)
         return RADM2_E_ARG;
+    if (o.placement == RADM2_PLACE_LU_TMEM && o.precision != RADM2_PREC_FP64) return RADM2_E_ARG;
     if (o.parity != 0 && o.parity != 1) return RADM2_E_ARG;
     if (o.cells_per_thread == 0) o.cells_per_thread = 1;
     if (o.cells_per_thread != 1 && o.cells_per_thread != 2) return RADM2_E_ARG;

@@ -51,7 +51,8 @@ cudaError_t launch_reduce(int n, const int *status, const int *nacc, const int *
 // (block size, placement, min resident blocks per SM) lists of the built solver variants,
 // per precision (each built for both schedules).  A min-blocks value above 1 caps the
 // registers per thread (65536 / (bs * minb)) for occupancy.
-#define RADM2_VARIANTS_FP64(X) X(32, 0, 1) X(64, 0, 1) X(128, 0, 1) X(256, 0, 1) X(128, 0, 3) X(128, 0, 4) X(32, 1, 1) X(32, 3, 1)
+#define RADM2_VARIANTS_FP64(X) X(32, 0, 1) X(64, 0, 1) X(128, 0, 1) X(256, 0, 1) X(128, 0, 3) X(128, 0, 4) X(32, 1, 1) X(32, 3, 1) \
+    X(128, 4, 1) X(256, 4, 1)
 #define RADM2_VARIANTS_FP32(X) X(64, 0, 1) X(128, 0, 1) X(256, 0, 1) X(128, 0, 3) X(128, 0, 4) X(32, 1, 1) X(64, 1, 1) X(32, 3, 1)
 // Reference-arithmetic FP64 solver (radm2_opts.parity): global placement only.
 #define RADM2_VARIANTS_FP64X(X) X(32, 0, 1) X(64, 0, 1) X(128, 0, 1) X(256, 0, 1)

@@ -27,11 +27,12 @@
 #pragma once
 
 #include "radm2_device.cuh"
+#include "gen/radm2_tmem.h"
 
 namespace radm2 {
 
 enum { SCHED_STATIC = 0, SCHED_PERSISTENT = 1 };
-enum { PLACE_GLOBAL = 0, PLACE_LU_SMEM = 1, PLACE_RCY_SMEM = 2 };
+enum { PLACE_GLOBAL = 0, PLACE_LU_SMEM = 1, PLACE_RCY_SMEM = 2, PLACE_LU_TMEM = 4 };
 
 constexpr int RCY_WORDS = NREACT + NVAR;  // 215
 constexpr int RCY_RC = 0, RCY_Y = NREACT;
@@ -135,6 +136,54 @@ inline int layout_check(int bs)
 #define RADM2_FUN_PHASE __noinline__
 #endif
 
+// ---------------------------------------------------------------- tensor-memory slots
+// PLACE_LU_TMEM keeps the RADM2_TMEM_SLOTS most accessed LU slots of every thread in tensor
+// memory instead of its global scratch: thread t of warp w owns lane 32 (w % 4) + t of its
+// CTA's allocation and 256 columns of it (the upper half of a 512-column allocation for warps
+// 4-7), a double in two 32-bit columns.  Tensor memory is separate from the L1 / shared
+// memory array, so it adds on-chip storage without shrinking the cache.  Its loads and stores
+// are warp-collective (.sync.aligned): every lane of the warp executes them together.
+
+// One double from tensor memory.  The thread's earlier stores are completed first (they may
+// be to the same columns), and the value is waited for inside the same statement, so it is
+// never read before it has arrived.
+__device__ __forceinline__ double tmem_ld_f64(uint32_t t)
+{
+    uint32_t lo, hi;
+    asm volatile(
+        "tcgen05.wait::st.sync.aligned;\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0, %1}, [%2];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
+        : "=r"(lo), "=r"(hi)
+        : "r"(t));
+    return __hiloint2double((int)hi, (int)lo);
+}
+
+__device__ __forceinline__ void tmem_st_f64(uint32_t t, double v)
+{
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x2.b32 [%0], {%1, %2};" ::"r"(t), "r"(__double2loint(v)),
+                 "r"(__double2hiint(v)));
+}
+
+// An LU slot held in tensor memory: reads load it, assignment stores it.
+struct TmemSlot {
+    uint32_t t;  // address of the slot's first column in the thread's lane
+    __device__ __forceinline__ operator double() const { return tmem_ld_f64(t); }
+    __device__ __forceinline__ void operator=(double v) const { tmem_st_f64(t, v); }
+};
+
+// Slot S of the thread's LU: its global (or shared) scratch word, or with TM its
+// tensor-memory columns when the slot is one of the tensor-memory slots.
+template <int TM, int BS, int S, typename LUT>
+__device__ __forceinline__ decltype(auto) lu_slot(LUT *sg, uint32_t tb)
+{
+    constexpr int col = radm2_tmem_col[S];
+    if constexpr (TM != 0 && col >= 0)
+        return TmemSlot{tb + (uint32_t)col};
+    else
+        return (sg[S * BS]);
+}
+
 // ---------------------------------------------------------------- phases
 // Each phase is a function of its own, inlined into the kernel (RADM2_PHASE) except the
 // RHS (RADM2_FUN_PHASE), which exists once in the instruction stream although both Fcn0
@@ -156,13 +205,14 @@ __device__ RADM2_FUN_PHASE void ph_fun(const double *v, const double *rc, double
 }
 
 // G = -J(y) + ghinv I in the LU slots (mgpu.cu:3139-3142 with the diagonal of 2700 restored).
-template <int BS, typename LUT>
-__device__ RADM2_PHASE void ph_jac(const double *y, const double *rc, LUT *sg, double fix0, double fix1, double ghinv)
+template <int BS, typename LUT, int TM = 0>
+__device__ RADM2_PHASE void ph_jac(const double *y, const double *rc, LUT *sg, double fix0, double fix1, double ghinv,
+                                   uint32_t tb = 0)
 {
 #define V(i) y[(i) * BS]
 #define RC(r) rc[(r) * BS]
 #define FIX(k) ((k) == 0 ? fix0 : fix1)
-#define G(s) sg[(s) * BS]
+#define G(s) lu_slot<TM, BS, (s)>(sg, tb)
 #define JAC_OUT(s, e) G(s) = (LUT)(-(e))
 #define JAC_OUT_DIAG(s, e) G(s) = (LUT)((-(e)) + ghinv)
 #define JAC_OUT_ZERO(s, d) G(s) = (d) ? (LUT)((-0.0) + ghinv) : (LUT)(-0.0)
@@ -178,17 +228,23 @@ __device__ RADM2_PHASE void ph_jac(const double *y, const double *rc, LUT *sg, d
 
 // In-place LU; returns 0 or the 1-based row of a zero pivot (checked before the row is
 // eliminated, as mgpu.cu:2753-2757 does).
-template <int BS, typename LUT>
-__device__ RADM2_PHASE int ph_decomp(LUT *sg)
+template <int BS, typename LUT, int TM = 0>
+__device__ RADM2_PHASE int ph_decomp(LUT *sg, uint32_t tb = 0)
 {
     int sing = 0;
-#define G(s) sg[(s) * BS]
+#define G(s) lu_slot<TM, BS, (s)>(sg, tb)
 #define LU_T LUT
 // One elimination step's loads may not be hoisted above the previous step: this bounds
 // the live set to one pivot row's worth of U entries and keeps the LU free of spills.
 #define LU_STEP_FENCE asm volatile("" ::: "memory")
-#define LU_PIVOT_CHECK(k, v) \
-    if (sing == 0 && (v) == (LUT)0) sing = (k) + 1
+// (tensor memory: the pivot is read on every lane, as its load is warp-collective)
+#define LU_PIVOT_CHECK(k, v)                                      \
+    if (TM) {                                                     \
+        const LUT pv_ = (v);                                      \
+        sing = (sing == 0 && pv_ == (LUT)0) ? (k) + 1 : sing;     \
+        __syncwarp();                                             \
+    } else if (sing == 0 && (v) == (LUT)0)                        \
+    sing = (k) + 1
 #include RADM2_DECOMP_INC
 #undef LU_PIVOT_CHECK
 #undef LU_STEP_FENCE
@@ -240,13 +296,14 @@ __device__ RADM2_PHASE int ph_jaclu(const double *y, const double *rc, LUT *sg, 
 // compiles the FP32 form without the refinement code (refine must be 0): the residual's
 // Jacobian-vector product and second substitution would otherwise stay in the kernel's
 // instruction footprint although they never run.
-template <int BS, typename LUT, int IR>
+template <int BS, typename LUT, int IR, int TM = 0>
 __device__ RADM2_PHASE void ph_stage(int stage, const double *y, const double *rc, double *vec, const LUT *sg,
                                       double fix0, double fix1, double hc21, double hc31, double hc32,
-                                      double ghinv, int refine)
+                                      double ghinv, int refine, uint32_t tb = 0)
 {
+    static_assert(TM == 0 || sizeof(LUT) == 8, "tensor-memory LU slots hold doubles");
 #define VW(w) vec[(w) * BS]
-#define G(s) sg[(s) * BS]
+#define G(s) lu_slot<TM, BS, (s)>(sg, tb)
     double x[NVAR];
     if (stage == 0) {
 #pragma unroll
@@ -323,6 +380,29 @@ template <int BS, typename LUT, int SCHED, int PLACE, int MINB, int IR = 1, int 
 __global__ void __launch_bounds__(BS, MINB) k_rosenbrock(const SolveArgs a)
 {
     using L = Layout<LUT, PLACE>;
+    constexpr int TM = (PLACE & PLACE_LU_TMEM) != 0;
+    static_assert(!TM || (sizeof(LUT) == 8 && (BS == 128 || BS == 256) && (PLACE & PLACE_LU_SMEM) == 0),
+                  "tensor-memory LU slots: FP64, 128 or 256 threads per block, LU otherwise in global scratch");
+    // Tensor memory: 256 columns per 128 threads (two CTAs of 128 or one of 256 fill an SM's
+    // 512 columns); warp 0 allocates them and gives up the right to allocate more.
+    constexpr uint32_t TCOLS = BS == 256 ? 512u : 256u;
+    uint32_t talloc = 0, tb = 0;  // the allocation, and this thread's first column in it
+    if constexpr (TM) {
+        __shared__ uint32_t tmem_base;
+        if (threadIdx.x < 32) {
+            asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                             (uint32_t)__cvta_generic_to_shared(&tmem_base)),
+                         "r"(TCOLS)
+                         : "memory");
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        talloc = tmem_base;
+        const uint32_t w = threadIdx.x >> 5;
+        tb = talloc + ((32u * (w & 3u)) << 16) + (w >> 2) * 256u;
+    }
     extern __shared__ double smem[];
     double *const gblk = a.scratch + (size_t)blockIdx.x * (L::global_words * BS);  // block bases
     double *const sblk = smem;
@@ -430,41 +510,52 @@ __global__ void __launch_bounds__(BS, MINB) k_rosenbrock(const SolveArgs a)
             outer = false;
         }
         if (!__any_sync(0xffffffffu, have)) break;
-        if (!have) continue;
+        if (!TM && !have) continue;
 
         // ---------------------------------------------------------------- one attempt
-        if (nstp >= P.max_steps) {
+        // With tensor-memory LU slots every lane of the warp runs the Jacobian, the LU and
+        // the stages together (their tensor-memory accesses are warp-collective); a lane
+        // without an attempt (act false) runs them on its own scratch and drops the result.
+        bool act = have;
+        if (act && nstp >= P.max_steps) {
             status = -6;
             done = true;
-            continue;
+            act = false;
         }
-        if ((T + 0.1 * H == T) || (H <= P.Roundoff)) {
+        if (act && ((T + 0.1 * H == T) || (H <= P.Roundoff))) {
             status = -7;
             done = true;
-            continue;
+            act = false;
         }
-        const double ghinv = 1.0 / (dir * H * RADM2_ROS_GAMMA0);
+        if (!TM && !act) continue;
+        const double Ha = act ? H : 1.0;
+        const double ghinv = 1.0 / (dir * Ha * RADM2_ROS_GAMMA0);
+        if (TM) __syncwarp();
         // G = -J(Y) + ghinv I in the LU slots, factored.
-#if RADM2_JACLU
-        const int sing = ph_jaclu<BS, LUT>(rcy + RCY_Y * BS, rcy + RCY_RC * BS, sg, fix0, fix1, ghinv);
-#else
-        ph_jac<BS, LUT>(rcy + RCY_Y * BS, rcy + RCY_RC * BS, sg, fix0, fix1, ghinv);
-        const int sing = ph_decomp<BS, LUT>(sg);
-#endif
-        if (sing) {
+        int sing;
+        if constexpr (TM || !RADM2_JACLU) {
+            ph_jac<BS, LUT, TM>(rcy + RCY_Y * BS, rcy + RCY_RC * BS, sg, fix0, fix1, ghinv, tb);
+            sing = ph_decomp<BS, LUT, TM>(sg, tb);
+        } else {
+            sing = ph_jaclu<BS, LUT>(rcy + RCY_Y * BS, rcy + RCY_RC * BS, sg, fix0, fix1, ghinv);
+        }
+        if (act && sing) {
             status = -8;
             done = true;
-            continue;
+            act = false;
         }
-        const double hc21 = RADM2_ROS_C0 / (dir * H);
-        const double hc31 = RADM2_ROS_C1 / (dir * H);
-        const double hc32 = RADM2_ROS_C2 / (dir * H);
+        if (!TM && !act) continue;
+        const double hc21 = RADM2_ROS_C0 / (dir * Ha);
+        const double hc31 = RADM2_ROS_C1 / (dir * Ha);
+        const double hc32 = RADM2_ROS_C2 / (dir * Ha);
 
 #pragma unroll 1
         for (int stage = 0; stage < 3; stage++) {
-            ph_stage<BS, LUT, IR>(stage, rcy + RCY_Y * BS, rcy + RCY_RC * BS, vec, sg, fix0, fix1, hc21, hc31, hc32, ghinv,
-                              a.refine);
+            if (TM) __syncwarp();
+            ph_stage<BS, LUT, IR, TM>(stage, rcy + RCY_Y * BS, rcy + RCY_RC * BS, vec, sg, fix0, fix1, hc21, hc31, hc32,
+                                      ghinv, a.refine, tb);
         }
+        if (!act) continue;
         nstp++;
 
         // Error norm and step control (mgpu.cu:3223-3260).
@@ -506,6 +597,15 @@ __global__ void __launch_bounds__(BS, MINB) k_rosenbrock(const SolveArgs a)
             nrej++;
             H = hnew;
         }
+    }
+    if constexpr (TM) {  // every warp is done with its tensor memory: warp 0 frees it
+        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (threadIdx.x < 32)
+            asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(talloc), "r"(TCOLS)
+                         : "memory");
     }
 #undef RW
 #undef VW

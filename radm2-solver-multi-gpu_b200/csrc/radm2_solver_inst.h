@@ -37,6 +37,8 @@ cudaError_t info_one(SolverInfo *out)
     int blocks = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k, BS, smem);
     if (e != cudaSuccess) return e;
+    // tensor-memory LU slots: 256 columns per 128 threads, 512 per SM
+    if ((PLACE & PLACE_LU_TMEM) && blocks * (BS / 128) > 2) blocks = 2 / (BS / 128);
     out->regs = at.numRegs;
     out->local_bytes = (int)at.localSizeBytes;
     out->blocks_per_sm = blocks;

@@ -380,6 +380,7 @@ def emit_cuda(m, out_dir):
         if not recip:
             flops["decomp"], flops["solve"] = fd, fs
         emit_jaclu(m, crow, diag, icol, nvar, out_dir, recip)
+    emit_tmem(crow, diag, icol, nvar, out_dir)
 
     h.append("\n/* Algorithmic flop counts per call, counted from the emitted expressions */\n")
     for k, v in sorted(flops.items()):
@@ -460,6 +461,49 @@ def emit_lu(crow, diag, icol, nvar, out_dir, recip):
         f += 1
     write(os.path.join(out_dir, "radm2_solve%s.inc" % sfx), body)
     return fdec, f
+
+
+TMEM_SLOTS = 128  # doubles of tensor memory per thread (256 32-bit columns)
+
+
+def lu_slot_accesses(crow, diag, icol, nvar):
+    """Loads and stores of each LU slot in one step attempt of the thread-per-cell solver:
+    the Jacobian's store, the factorisation's row loads, stores and pivot-row reads
+    (emit_lu's order; a row without eliminations touches only its pivot), and the three
+    stage solves' reads."""
+    acc = [1] * len(icol)
+    for k in range(nvar):
+        if crow[k] == diag[k]:
+            acc[diag[k]] += 2
+            continue
+        for s in range(crow[k], crow[k + 1]):
+            acc[s] += 2
+        for kk in range(crow[k], diag[k]):
+            j = icol[kk]
+            acc[diag[j]] += 1
+            for jj in range(diag[j] + 1, crow[j + 1]):
+                acc[jj] += 1
+    for k in range(nvar):
+        for s in range(crow[k], crow[k + 1]):
+            acc[s] += 3
+    return acc
+
+
+def emit_tmem(crow, diag, icol, nvar, out_dir):
+    """The LU slots a thread keeps in its tensor-memory row: the TMEM_SLOTS most accessed
+    per step attempt (ties by slot index), each a double in two 32-bit columns."""
+    acc = lu_slot_accesses(crow, diag, icol, nvar)
+    hot = sorted(range(len(icol)), key=lambda s: (-acc[s], s))[:TMEM_SLOTS]
+    col = [-1] * len(icol)
+    for i, s in enumerate(sorted(hot)):
+        col[s] = 2 * i
+    body = [BANNER, "/* Tensor-memory placement of the LU slots (PLACE_LU_TMEM): the %d slots with the\n"
+            " * most loads and stores per step attempt (%d of %d), slot s at 32-bit column\n"
+            " * radm2_tmem_col[s] of the thread's row, -1: global scratch. */\n"
+            % (TMEM_SLOTS, sum(acc[s] for s in hot), sum(acc)),
+            "#pragma once\n#define RADM2_TMEM_SLOTS %d\n" % TMEM_SLOTS,
+            "static constexpr short radm2_tmem_col[%d] = {%s};\n" % (len(col), ",".join(map(str, col)))]
+    write(os.path.join(out_dir, "radm2_tmem.h"), body)
 
 
 def slot_chain(t):
