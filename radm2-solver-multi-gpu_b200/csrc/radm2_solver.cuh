@@ -217,6 +217,7 @@ __device__ RADM2_PHASE void ph_jac(const double *y, const double *rc, LUT *sg, d
 #define JAC_OUT_DIAG(s, e) G(s) = (LUT)((-(e)) + ghinv)
 #define JAC_OUT_ZERO(s, d) G(s) = (d) ? (LUT)((-0.0) + ghinv) : (LUT)(-0.0)
 #include "gen/radm2_jac.inc"
+    if constexpr (TM) asm volatile("tcgen05.wait::st.sync.aligned;");  // stores done before the LU reads
 #undef JAC_OUT
 #undef JAC_OUT_DIAG
 #undef JAC_OUT_ZERO
@@ -245,7 +246,13 @@ __device__ RADM2_PHASE int ph_decomp(LUT *sg, uint32_t tb = 0)
         __syncwarp();                                             \
     } else if (sing == 0 && (v) == (LUT)0)                        \
     sing = (k) + 1
+    if constexpr (TM) {  // tensor-memory slots read and written in groups
+#define TM_BASE tb
+#include "gen/radm2_decomp_rcp_tm.inc"
+#undef TM_BASE
+    } else {
 #include RADM2_DECOMP_INC
+    }
 #undef LU_PIVOT_CHECK
 #undef LU_STEP_FENCE
 #undef LU_T
@@ -322,7 +329,13 @@ __device__ RADM2_PHASE void ph_stage(int stage, const double *y, const double *r
 #pragma unroll
         for (int i = 0; i < NVAR; i++) x[i] = VW(VEC_K3 + i) + VW(VEC_K2 + i) * hc32;
     }
-    if (sizeof(LUT) == 8) {
+    if constexpr (TM) {
+#define X(i) x[i]
+#define TM_BASE tb
+#include "gen/radm2_solve_rcp_tm.inc"
+#undef TM_BASE
+#undef X
+    } else if (sizeof(LUT) == 8) {
 #define X(i) x[i]
 #include RADM2_SOLVE_INC
 #undef X

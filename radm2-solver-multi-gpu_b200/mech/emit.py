@@ -380,7 +380,8 @@ def emit_cuda(m, out_dir):
         if not recip:
             flops["decomp"], flops["solve"] = fd, fs
         emit_jaclu(m, crow, diag, icol, nvar, out_dir, recip)
-    emit_tmem(crow, diag, icol, nvar, out_dir)
+    tcol = emit_tmem(crow, diag, icol, nvar, out_dir)
+    emit_lu_tm(crow, diag, icol, nvar, tcol, out_dir)
 
     h.append("\n/* Algorithmic flop counts per call, counted from the emitted expressions */\n")
     for k, v in sorted(flops.items()):
@@ -504,6 +505,188 @@ def emit_tmem(crow, diag, icol, nvar, out_dir):
             "#pragma once\n#define RADM2_TMEM_SLOTS %d\n" % TMEM_SLOTS,
             "static constexpr short radm2_tmem_col[%d] = {%s};\n" % (len(col), ",".join(map(str, col)))]
     write(os.path.join(out_dir, "radm2_tmem.h"), body)
+    return col
+
+
+TM_GROUP = 16  # doubles per tensor-memory load statement (32 registers)
+
+
+def tm_runs(slots, col):
+    """Split a list of slots into runs of tensor-memory slots with consecutive columns
+    (global slots are left out)."""
+    runs, cur = [], []
+    for s in slots:
+        if col[s] >= 0 and cur and col[s] == col[cur[-1]] + 2:
+            cur.append(s)
+        else:
+            if cur:
+                runs.append(cur)
+            cur = [s] if col[s] >= 0 else []
+    if cur:
+        runs.append(cur)
+    return runs
+
+
+def tm_pieces(run, col):
+    """A run as (first slot index in the run, doubles) pieces of 1, 2, 4 or 8 doubles, each
+    starting on a column that is a multiple of its own width."""
+    out, i = [], 0
+    while i < len(run):
+        c = col[run[i]]
+        for p in (8, 4, 2, 1):
+            if p <= len(run) - i and c % (2 * p) == 0:
+                out.append((i, p))
+                i += p
+                break
+    return out
+
+
+def tm_load(pairs, col, ind):
+    """Load tensor-memory slots into already declared doubles: pairs [(slot, var)] in slot
+    order.  One statement per TM_GROUP doubles: its loads, then one wait, so the values are
+    never read before they arrive."""
+    var = dict(pairs)
+    pieces = []
+    for run in tm_runs([s for s, _ in pairs], col):
+        pieces += [(run[i:i + p], p) for i, p in tm_pieces(run, col)]
+    lines, group, n = [], [], 0
+    for pc in pieces + [None]:
+        if pc is None or n + pc[1] > TM_GROUP:
+            if group:
+                nout = 2 * n
+                text, outs, ins, k = [], [], [], 0
+                for gi, (sl, p) in enumerate(group):
+                    regs = ",".join("%%%d" % (k + r) for r in range(2 * p))
+                    text.append("tcgen05.ld.sync.aligned.32x32b.x%d.b32 {%s}, [%%%d];" % (2 * p, regs, nout + gi))
+                    for s in sl:
+                        outs.append('"=r"(tl%d), "=r"(th%d)' % (s, s))
+                    ins.append('"r"(TM_BASE + %du)' % col[sl[0]])
+                    k += 2 * p
+                text.append("tcgen05.wait::ld.sync.aligned;")
+                slots = [s for sl, _ in group for s in sl]
+                lines.append("%s{ unsigned %s;\n" % (ind, ", ".join("tl%d, th%d" % (s, s) for s in slots)))
+                lines.append('%s  asm volatile("%s" : %s : %s);\n' % (ind, "\\n\\t".join(text), ", ".join(outs),
+                                                                      ", ".join(ins)))
+                for s in slots:
+                    lines.append("%s  %s = __hiloint2double((int)th%d, (int)tl%d);\n" % (ind, var[s], s, s))
+                lines.append("%s}\n" % ind)
+            group, n = [], 0
+        if pc is not None:
+            group.append(pc)
+            n += pc[1]
+    return lines
+
+
+def tm_store(pairs, col, ind):
+    """Store doubles into tensor-memory slots: pairs [(slot, expression)] in slot order.
+    The stores are asynchronous; the caller waits for them before the slots are read."""
+    val = dict(pairs)
+    lines = []
+    for run in tm_runs([s for s, _ in pairs], col):
+        for i, p in tm_pieces(run, col):
+            sl = run[i:i + p]
+            regs = ",".join("%%%d" % (1 + r) for r in range(2 * p))
+            ins = ['"r"(TM_BASE + %du)' % col[sl[0]]]
+            for s in sl:
+                ins.append('"r"(__double2loint(%s)), "r"(__double2hiint(%s))' % (val[s], val[s]))
+            lines.append('%sasm volatile("tcgen05.st.sync.aligned.32x32b.x%d.b32 [%%0], {%s};" :: %s);\n'
+                         % (ind, 2 * p, regs, ", ".join(ins)))
+    return lines
+
+
+def emit_lu_tm(crow, diag, icol, nvar, col, out_dir):
+    """The reciprocal-pivot LU and triangular solves of emit_lu for the tensor-memory
+    placement: the same operations in the same order, with the tensor-memory slots of a row
+    (or of a pivot row's U part) read by wide tcgen05 loads with one wait per group instead
+    of one load and one wait each.  Global slots go through G(s).  TM_BASE is the thread's
+    first column address; every statement is warp-collective."""
+    body = [BANNER, "/* Pivot-free LU (mgpu.cu:2746-2779 order, reciprocal pivots) with tensor-memory slots\n"
+            " * (radm2_tmem.h) loaded and stored in groups.  Accessors: G(s) (global slots), LU_T,\n"
+            " * TM_BASE, LU_PIVOT_CHECK(row, value), LU_STEP_FENCE. */\n",
+            "#ifndef LU_STEP_FENCE\n#define LU_STEP_FENCE do { } while (0)\n#endif\n"]
+    wait_st = '  asm volatile("tcgen05.wait::st.sync.aligned;");\n'
+    since_fence = 0
+    for k in range(nvar):
+        body.append("{ /* row %d */\n" % k)
+        d = diag[k]
+        if crow[k] == d:
+            if col[d] >= 0:
+                body.append("  LU_T w%d;\n" % k)
+                body += tm_load([(d, "w%d" % k)], col, "  ")
+                body.append("  LU_PIVOT_CHECK(%d, w%d);\n" % (k, k))
+                body += tm_store([(d, "((LU_T)1 / w%d)" % k)], col, "  ")
+                body.append(wait_st)
+            else:
+                body.append("  LU_PIVOT_CHECK(%d, G(%d));\n" % (k, d))
+                body.append("  G(%d) = (LU_T)1 / G(%d);\n" % (d, d))
+            body.append("}\n")
+            continue
+        row = list(range(crow[k], crow[k + 1]))
+        for sl in row:
+            if col[sl] >= 0:
+                body.append("  LU_T w%d;\n" % icol[sl])
+            else:
+                body.append("  LU_T w%d = G(%d);\n" % (icol[sl], sl))
+        body += tm_load([(sl, "w%d" % icol[sl]) for sl in row if col[sl] >= 0], col, "  ")
+        body.append("  LU_PIVOT_CHECK(%d, w%d);\n" % (k, k))
+        for kk in range(crow[k], d):
+            j = icol[kk]
+            seg = [diag[j]] + list(range(diag[j] + 1, crow[j + 1]))
+            tms = [s for s in seg if col[s] >= 0]
+            body.append("  {\n")
+            if tms:
+                body.append("    LU_T %s;\n" % ", ".join("u%d" % s for s in tms))
+                body += tm_load([(s, "u%d" % s) for s in tms], col, "    ")
+            ref = lambda s: ("u%d" % s) if col[s] >= 0 else ("G(%d)" % s)  # noqa: E731
+            body.append("    const LU_T a = -w%d * %s; w%d = -a;\n" % (j, ref(diag[j]), j))
+            for jj in range(diag[j] + 1, crow[j + 1]):
+                body.append("    w%d += a * %s;\n" % (icol[jj], ref(jj)))
+            since_fence += crow[j + 1] - diag[j]
+            if since_fence >= LU_FENCE_LOADS:
+                body.append("  LU_STEP_FENCE;\n")
+                since_fence = 0
+            body.append("  }\n")
+        out = []
+        for sl in row:
+            v = "((LU_T)1 / w%d)" % icol[sl] if sl == d else "w%d" % icol[sl]
+            if col[sl] >= 0:
+                out.append((sl, v))
+            else:
+                body.append("  G(%d) = %s;\n" % (sl, v))
+        if out:
+            body += tm_store(out, col, "  ")
+            body.append(wait_st)
+        body.append("}\n")
+    write(os.path.join(out_dir, "radm2_decomp_rcp_tm.inc"), body)
+
+    body = [BANNER, "/* Solve (LU) x = b in place on X(i) (mgpu.cu:2873-3090 order, reciprocal pivots)\n"
+            " * with tensor-memory slots loaded in groups.  Accessors: G(s), X(i), TM_BASE. */\n"]
+    for k in range(nvar):
+        if crow[k] == diag[k]:
+            continue
+        seg = list(range(crow[k], diag[k]))
+        tms = [s for s in seg if col[s] >= 0]
+        body.append("{\n")
+        if tms:
+            body.append("  double %s;\n" % ", ".join("g%d" % s for s in tms))
+            body += tm_load([(s, "g%d" % s) for s in tms], col, "  ")
+        expr = "X(%d)" % k
+        for sl in seg:
+            expr = "(%s - %s * X(%d))" % (expr, ("g%d" % sl) if col[sl] >= 0 else ("G(%d)" % sl), icol[sl])
+        body.append("  X(%d) = %s;\n}\n" % (k, expr))
+    for k in reversed(range(nvar)):
+        seg = [diag[k]] + list(range(diag[k] + 1, crow[k + 1]))
+        tms = [s for s in seg if col[s] >= 0]
+        body.append("{\n")
+        if tms:
+            body.append("  double %s;\n" % ", ".join("g%d" % s for s in tms))
+            body += tm_load([(s, "g%d" % s) for s in tms], col, "  ")
+        ref = lambda s: ("g%d" % s) if col[s] >= 0 else ("G(%d)" % s)  # noqa: E731
+        expr = "X(%d)" % k
+        for sl in range(diag[k] + 1, crow[k + 1]):
+            expr = "(%s - %s * X(%d))" % (expr, ref(sl), icol[sl])
+        body.append("  X(%d) = %s * %s;\n}\n" % (k, expr, ref(diag[k])))
+    write(os.path.join(out_dir, "radm2_solve_rcp_tm.inc"), body)
 
 
 def slot_chain(t):
