@@ -276,12 +276,14 @@ def per_species_errors(y, ref):
 
 def solver_kernel_name(tuned, args):
     """The solver kernel the timed arm launched (after autotuning, if any)."""
-    sched, bs = args.schedule, args.block_threads
+    sched, bs, place = args.schedule, args.block_threads, PLACEMENTS[args.placement]
     if tuned is not None:
         sched, bs = SCHED_NAMES[tuned["chosen"]["schedule"]], tuned["chosen"]["block_threads"]
+        place = tuned["chosen"]["placement"]
     if sched == "coop":
         return "k_rosenbrock_coop%s_g%d (cooperative solver)" % ("x" if args.parity else "", (bs or 256) // 32)
-    return "k_rosenbrock (thread-per-cell solver, %s)" % sched
+    return "k_rosenbrock (thread-per-cell solver, %s%s)" % (
+        sched, ", LU slots in tensor memory" if place == PLACEMENTS["lu-tmem"] else "")
 
 
 def rel_errors(y, ref):
@@ -589,10 +591,13 @@ def main():
     if os.path.exists(tfile):
         with open(tfile) as f:
             tr = json.load(f)
-        sched_used = args.schedule
+        sched_used, place_used = args.schedule, PLACEMENTS[args.placement]
         if main_arm["tuned"] is not None:
             sched_used = SCHED_NAMES[main_arm["tuned"]["chosen"]["schedule"]]
+            place_used = main_arm["tuned"]["chosen"]["placement"]
         key = "%s-%s" % (args.precision, sched_used)
+        if place_used == PLACEMENTS["lu-tmem"]:
+            key += "-tmem"
         if key + "-" + wl in tr:  # a capture of this workload family, if there is one
             key = key + "-" + wl
         if key in tr:
