@@ -77,9 +77,9 @@ struct SolverInfo {
 };
 
 // Solver kernels: one launcher per (precision, schedule) file, variant key
-// bs * 64 + min_blocks * 4 + place (place: bit 0 = LU in shared memory, bit 1 = rate
-// constants and state in shared memory).
-inline int variant_key(int bs, int place, int min_blocks) { return bs * 64 + min_blocks * 4 + place; }
+// bs * 64 + min_blocks * 8 + place (place: bit 0 = LU in shared memory, bit 1 = rate
+// constants and state in shared memory, bit 2 = LU slots in tensor memory; min_blocks <= 4).
+inline int variant_key(int bs, int place, int min_blocks) { return bs * 64 + min_blocks * 8 + place; }
 cudaError_t launch_solver_fp64_static(const SolveArgs &a, int key, int grid, cudaStream_t st);
 cudaError_t launch_solver_fp64_persistent(const SolveArgs &a, int key, int grid, cudaStream_t st);
 cudaError_t launch_solver_fp32_static(const SolveArgs &a, int key, int grid, cudaStream_t st);

@@ -66,7 +66,7 @@ int check_one()
 #define RADM2_ARITH 0
 #endif
 
-#define RADM2_KEY(BS_, PL_, MB_) ((BS_) * 64 + (MB_) * 4 + (PL_))
+#define RADM2_KEY(BS_, PL_, MB_) ((BS_) * 64 + (MB_) * 8 + (PL_))  // = variant_key
 #define RADM2_CASE_LAUNCH(BS_, PL_, MB_) \
     case RADM2_KEY(BS_, PL_, MB_): return launch_one<BS_, RADM2_T, RADM2_S, PL_, MB_, RADM2_IR, RADM2_ARITH>(a, grid, st);
 #define RADM2_CASE_INFO(BS_, PL_, MB_) \
