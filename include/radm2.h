@@ -81,7 +81,7 @@ typedef struct radm2_opts {
 #define RADM2_PLACE_LU_SMEM 1  /* LU in shared memory (32 or 64 threads per block) */
 #define RADM2_PLACE_ALL_SMEM 3 /* LU, rate constants and state in shared memory (32 threads) */
 #define RADM2_PLACE_LU_TMEM 4  /* the 128 most used LU slots in tensor memory, the rest global
-                                  (FP64, 128 or 256 threads per block) */
+                                  (FP64, 128 or 256 threads per block; with parity, 256) */
 
 typedef struct radm2_ctx radm2_ctx;
 

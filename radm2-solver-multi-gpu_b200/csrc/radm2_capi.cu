@@ -505,7 +505,9 @@ int radm2_create(radm2_ctx **out, const radm2_opts *opts)
     if (o.cells_per_thread == 2 && (o.precision != RADM2_PREC_FP64 || o.placement != RADM2_PLACE_GLOBAL ||
                                     o.min_blocks > 1 || o.parity || o.schedule == RADM2_SCHED_COOP))
         return RADM2_E_ARG;
-    if (o.parity && (o.precision != RADM2_PREC_FP64 || o.placement != RADM2_PLACE_GLOBAL)) return RADM2_E_ARG;
+    if (o.parity && (o.precision != RADM2_PREC_FP64 ||
+                     (o.placement != RADM2_PLACE_GLOBAL && o.placement != RADM2_PLACE_LU_TMEM)))
+        return RADM2_E_ARG;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= o.device || o.device < 0) return RADM2_E_NODEV;
     cudaDeviceProp prop;

@@ -89,10 +89,14 @@ inline int layout_check(int bs)
 #define RADM2_LU_RECIP 1
 #endif
 #if RADM2_LU_RECIP
+#define RADM2_DECOMP_TM_INC "gen/radm2_decomp_rcp_tm.inc"
+#define RADM2_SOLVE_TM_INC "gen/radm2_solve_rcp_tm.inc"
 #define RADM2_DECOMP_INC "gen/radm2_decomp_rcp.inc"
 #define RADM2_JACLU_INC "gen/radm2_jaclu_rcp.inc"
 #define RADM2_SOLVE_INC "gen/radm2_solve_rcp.inc"
 #else
+#define RADM2_DECOMP_TM_INC "gen/radm2_decomp_tm.inc"
+#define RADM2_SOLVE_TM_INC "gen/radm2_solve_tm.inc"
 #define RADM2_DECOMP_INC "gen/radm2_decomp.inc"
 #define RADM2_JACLU_INC "gen/radm2_jaclu.inc"
 #define RADM2_SOLVE_INC "gen/radm2_solve.inc"
@@ -248,7 +252,7 @@ __device__ RADM2_PHASE int ph_decomp(LUT *sg, uint32_t tb = 0)
     sing = (k) + 1
     if constexpr (TM) {  // tensor-memory slots read and written in groups
 #define TM_BASE tb
-#include "gen/radm2_decomp_rcp_tm.inc"
+#include RADM2_DECOMP_TM_INC
 #undef TM_BASE
     } else {
 #include RADM2_DECOMP_INC
@@ -332,7 +336,7 @@ __device__ RADM2_PHASE void ph_stage(int stage, const double *y, const double *r
     if constexpr (TM) {
 #define X(i) x[i]
 #define TM_BASE tb
-#include "gen/radm2_solve_rcp_tm.inc"
+#include RADM2_SOLVE_TM_INC
 #undef TM_BASE
 #undef X
     } else if (sizeof(LUT) == 8) {

@@ -381,7 +381,8 @@ def emit_cuda(m, out_dir):
             flops["decomp"], flops["solve"] = fd, fs
         emit_jaclu(m, crow, diag, icol, nvar, out_dir, recip)
     tcol = emit_tmem(crow, diag, icol, nvar, out_dir)
-    emit_lu_tm(crow, diag, icol, nvar, tcol, out_dir)
+    for recip in (False, True):
+        emit_lu_tm(crow, diag, icol, nvar, tcol, out_dir, recip)
 
     h.append("\n/* Algorithmic flop counts per call, counted from the emitted expressions */\n")
     for k, v in sorted(flops.items()):
@@ -594,31 +595,35 @@ def tm_store(pairs, col, ind):
     return lines
 
 
-def emit_lu_tm(crow, diag, icol, nvar, col, out_dir):
-    """The reciprocal-pivot LU and triangular solves of emit_lu for the tensor-memory
-    placement: the same operations in the same order, with the tensor-memory slots of a row
-    (or of a pivot row's U part) read by wide tcgen05 loads with one wait per group instead
-    of one load and one wait each.  Global slots go through G(s).  TM_BASE is the thread's
-    first column address; every statement is warp-collective."""
-    body = [BANNER, "/* Pivot-free LU (mgpu.cu:2746-2779 order, reciprocal pivots) with tensor-memory slots\n"
+def emit_lu_tm(crow, diag, icol, nvar, col, out_dir, recip):
+    """The LU and triangular solves of emit_lu (reciprocal or division form) for the
+    tensor-memory placement: the same operations in the same order, with the tensor-memory
+    slots of a row (or of a pivot row's U part) read by wide tcgen05 loads with one wait per
+    group instead of one load and one wait each.  Global slots go through G(s).  TM_BASE is
+    the thread's first column address; every statement is warp-collective."""
+    sfx = "_rcp" if recip else ""
+    body = [BANNER, "/* Pivot-free LU (mgpu.cu:2746-2779 order, %s) with tensor-memory slots\n"
             " * (radm2_tmem.h) loaded and stored in groups.  Accessors: G(s) (global slots), LU_T,\n"
-            " * TM_BASE, LU_PIVOT_CHECK(row, value), LU_STEP_FENCE. */\n",
+            " * TM_BASE, LU_PIVOT_CHECK(row, value), LU_STEP_FENCE. */\n"
+            % ("reciprocal pivots" if recip else "pivot divisions"),
             "#ifndef LU_STEP_FENCE\n#define LU_STEP_FENCE do { } while (0)\n#endif\n"]
     wait_st = '  asm volatile("tcgen05.wait::st.sync.aligned;");\n'
     since_fence = 0
     for k in range(nvar):
         body.append("{ /* row %d */\n" % k)
         d = diag[k]
-        if crow[k] == d:
+        if crow[k] == d:  # no elimination: the pivot check, and in reciprocal form 1/pivot
             if col[d] >= 0:
                 body.append("  LU_T w%d;\n" % k)
                 body += tm_load([(d, "w%d" % k)], col, "  ")
                 body.append("  LU_PIVOT_CHECK(%d, w%d);\n" % (k, k))
-                body += tm_store([(d, "((LU_T)1 / w%d)" % k)], col, "  ")
-                body.append(wait_st)
+                if recip:
+                    body += tm_store([(d, "((LU_T)1 / w%d)" % k)], col, "  ")
+                    body.append(wait_st)
             else:
                 body.append("  LU_PIVOT_CHECK(%d, G(%d));\n" % (k, d))
-                body.append("  G(%d) = (LU_T)1 / G(%d);\n" % (d, d))
+                if recip:
+                    body.append("  G(%d) = (LU_T)1 / G(%d);\n" % (d, d))
             body.append("}\n")
             continue
         row = list(range(crow[k], crow[k + 1]))
@@ -638,7 +643,7 @@ def emit_lu_tm(crow, diag, icol, nvar, col, out_dir):
                 body.append("    LU_T %s;\n" % ", ".join("u%d" % s for s in tms))
                 body += tm_load([(s, "u%d" % s) for s in tms], col, "    ")
             ref = lambda s: ("u%d" % s) if col[s] >= 0 else ("G(%d)" % s)  # noqa: E731
-            body.append("    const LU_T a = -w%d * %s; w%d = -a;\n" % (j, ref(diag[j]), j))
+            body.append("    const LU_T a = -w%d %s %s; w%d = -a;\n" % (j, "*" if recip else "/", ref(diag[j]), j))
             for jj in range(diag[j] + 1, crow[j + 1]):
                 body.append("    w%d += a * %s;\n" % (icol[jj], ref(jj)))
             since_fence += crow[j + 1] - diag[j]
@@ -648,7 +653,7 @@ def emit_lu_tm(crow, diag, icol, nvar, col, out_dir):
             body.append("  }\n")
         out = []
         for sl in row:
-            v = "((LU_T)1 / w%d)" % icol[sl] if sl == d else "w%d" % icol[sl]
+            v = "((LU_T)1 / w%d)" % icol[sl] if (recip and sl == d) else "w%d" % icol[sl]
             if col[sl] >= 0:
                 out.append((sl, v))
             else:
@@ -657,10 +662,11 @@ def emit_lu_tm(crow, diag, icol, nvar, col, out_dir):
             body += tm_store(out, col, "  ")
             body.append(wait_st)
         body.append("}\n")
-    write(os.path.join(out_dir, "radm2_decomp_rcp_tm.inc"), body)
+    write(os.path.join(out_dir, "radm2_decomp%s_tm.inc" % sfx), body)
 
-    body = [BANNER, "/* Solve (LU) x = b in place on X(i) (mgpu.cu:2873-3090 order, reciprocal pivots)\n"
-            " * with tensor-memory slots loaded in groups.  Accessors: G(s), X(i), TM_BASE. */\n"]
+    body = [BANNER, "/* Solve (LU) x = b in place on X(i) (mgpu.cu:2873-3090 order, %s)\n"
+            " * with tensor-memory slots loaded in groups.  Accessors: G(s), X(i), TM_BASE. */\n"
+            % ("reciprocal pivots" if recip else "pivot divisions")]
     for k in range(nvar):
         if crow[k] == diag[k]:
             continue
@@ -685,8 +691,8 @@ def emit_lu_tm(crow, diag, icol, nvar, col, out_dir):
         expr = "X(%d)" % k
         for sl in range(diag[k] + 1, crow[k + 1]):
             expr = "(%s - %s * X(%d))" % (expr, ref(sl), icol[sl])
-        body.append("  X(%d) = %s * %s;\n}\n" % (k, expr, ref(diag[k])))
-    write(os.path.join(out_dir, "radm2_solve_rcp_tm.inc"), body)
+        body.append("  X(%d) = %s %s %s;\n}\n" % (k, expr, "*" if recip else "/", ref(diag[k])))
+    write(os.path.join(out_dir, "radm2_solve%s_tm.inc" % sfx), body)
 
 
 def slot_chain(t):

@@ -112,16 +112,36 @@ def test_tmem_split_graph_and_host_pipeline():
     assert rel_err(outs[1][1], outs[0][1]).max() <= 1e-12
 
 
+def test_tmem_reference_arithmetic(mixed4k):
+    """Reference arithmetic (radm2_opts.parity: pivot divisions, no multiply-add contraction)
+    with tensor-memory slots: the division-form fragments give the global-scratch parity
+    kernel's results bit for bit, and the oracle's within 1e-10 with identical step counts."""
+    opts = dict(schedule=radm2b200.SCHED_PERSISTENT, block_threads=256, parity=1)
+    ierr0, y0, st0, rc, _ = run(mixed4k, **opts)
+    ierr, y, st, _, _ = run(mixed4k, placement=TMEM, **opts)
+    assert ierr == ierr0 == 1
+    assert np.array_equal(y, y0) and np.array_equal(st["nacc"], st0["nacc"])
+    ipar, rpar = radm2b200.default_params(hstart=6.0)
+    ok, p = oracle.params(0.0, 600.0, ATOL, RTOL, rpar, ipar)
+    y_o, st_o = oracle.integrate(mixed4k["VAR"], mixed4k["FIX"], rc, p)
+    assert np.array_equal(st["nacc"], st_o["nacc"]) and np.array_equal(st["nrej"], st_o["nrej"])
+    e = rel_err(y, y_o).max()
+    print("reference arithmetic, tensor-memory LU slots, vs oracle: max %.2e" % e)
+    assert e <= PARITY
+
+
 def test_tmem_options():
-    """Tensor-memory slots exist for the FP64 fast solver with 128 or 256 threads per block."""
-    for bad in ({"precision": radm2b200.PREC_FP32LU}, {"parity": 1}, {"schedule": radm2b200.SCHED_COOP},
+    """Tensor-memory slots exist for the FP64 solvers with 128 or 256 threads per block (256
+    for reference arithmetic)."""
+    for bad in ({"precision": radm2b200.PREC_FP32LU}, {"schedule": radm2b200.SCHED_COOP},
                 {"cells_per_thread": 2}):
         with pytest.raises(radm2b200.RadmError):
             radm2b200.Solver(**dict({"placement": TMEM}, **bad))
     cells = inputs.make_cells(64, 1, "plain")
-    with radm2b200.Solver(placement=TMEM, block_threads=64) as s:
-        s.set_cells(cells)
-        ipar, rpar = radm2b200.default_params()
-        assert s.rosenbrock(0.0, 600.0, ATOL, RTOL, rpar, ipar) == radm2b200.lib.RADM2_E_ARG  # not built for 64
+    for shape in ({"block_threads": 64}, {"block_threads": 128, "parity": 1}):  # not built
+        with radm2b200.Solver(placement=TMEM, **shape) as s:
+            s.set_cells(cells)
+            ipar, rpar = radm2b200.default_params()
+            assert s.rosenbrock(0.0, 600.0, ATOL, RTOL, rpar, ipar) == radm2b200.lib.RADM2_E_ARG
     with radm2b200.Solver(placement=TMEM) as s:
         assert s.opts()["block_threads"] in (0, 128) and s.opts()["placement"] == TMEM

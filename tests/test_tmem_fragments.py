@@ -1,5 +1,6 @@
-"""The tensor-memory LU and solve fragments (csrc/gen/radm2_{decomp,solve}_rcp_tm.inc) against
-the plain ones they stand in for, read as text on the CPU.
+"""The tensor-memory LU and solve fragments (csrc/gen/radm2_{decomp,solve}{_rcp,}_tm.inc: the
+reciprocal-pivot and the division form) against the plain ones they stand in for, read as text
+on the CPU.
 
 - Every tcgen05 load and store piece covers exactly its slots' columns (radm2_tmem.h): in
   slot order, two 32-bit columns per double, starting on a multiple of its own width, inside
@@ -10,6 +11,7 @@ the plain ones they stand in for, read as text on the CPU.
 import os
 import re
 
+import pytest
 from conftest import PKG
 
 GEN = os.path.join(PKG, "csrc", "gen")
@@ -30,9 +32,13 @@ COL = tmem_cols()
 PIECE = re.compile(r"tcgen05\.(ld|st)\.sync\.aligned\.32x32b\.x(\d+)\.b32")
 
 
-def test_load_and_store_pieces_cover_their_columns():
+FORMS = ["_rcp", ""]  # reciprocal pivots (the fast solver), divisions (reference arithmetic)
+
+
+@pytest.mark.parametrize("form", FORMS)
+def test_load_and_store_pieces_cover_their_columns(form):
     n = 0
-    for name in ("radm2_decomp_rcp_tm.inc", "radm2_solve_rcp_tm.inc"):
+    for name in ("radm2_decomp%s_tm.inc" % form, "radm2_solve%s_tm.inc" % form):
         for line in read(name).splitlines():
             if "tcgen05.ld" in line:
                 widths = [int(w) for op, w in PIECE.findall(line)]
@@ -82,9 +88,10 @@ def normalise(text):
     return out
 
 
-def test_solves_are_the_plain_solves():
-    plain = [s for s in normalise(read("radm2_solve_rcp.inc"))]
-    tm = normalise(read("radm2_solve_rcp_tm.inc"))
+@pytest.mark.parametrize("form", FORMS)
+def test_solves_are_the_plain_solves(form):
+    plain = [s for s in normalise(read("radm2_solve%s.inc" % form))]
+    tm = normalise(read("radm2_solve%s_tm.inc" % form))
     assert tm == plain
 
 
@@ -109,8 +116,9 @@ def stores_by_row(text, tm):
     return rows
 
 
-def test_factorisation_is_the_plain_factorisation():
-    plain_text, tm_text = read("radm2_decomp_rcp.inc"), read("radm2_decomp_rcp_tm.inc")
+@pytest.mark.parametrize("form", FORMS)
+def test_factorisation_is_the_plain_factorisation(form):
+    plain_text, tm_text = read("radm2_decomp%s.inc" % form), read("radm2_decomp%s_tm.inc" % form)
     elim = lambda lines: [s for s in lines if "const LU_T a =" in s or "+= a *" in s]  # noqa: E731
     assert elim(normalise(tm_text)) == elim(normalise(plain_text))
     sp, st = stores_by_row(plain_text, False), stores_by_row(tm_text, True)
