@@ -70,7 +70,9 @@ WORKLOADS = {
 ATOL, RTOL, RTOL_TIGHT = 1.0, 1.0e-3, 1.0e-8
 SCHED_NAMES = {0: "static", 1: "persistent", 2: "coop"}
 # --placement names -> RADM2_PLACE_* (include/radm2.h)
-PLACEMENTS = {"": 0, "global": 0, "lu-smem": 1, "all-smem": 3, "lu-tmem": 4}
+PLACEMENTS = {"": 0, "global": 0, "lu-smem": 1, "all-smem": 3, "lu-tmem": 4, "lu-tmem-wide": 10}
+TMEM_NAMES = {4: ", LU slots in tensor memory",
+              10: ", 256 LU slots per thread in tensor memory, rate constants and state in shared memory"}
 
 
 # HBM copy bandwidth of a B200 when no measured peak file is present (GB/s).
@@ -93,7 +95,7 @@ def parse():
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shape")
     ap.add_argument("--block-threads", type=int, default=0)
     ap.add_argument("--blocks-per-sm", type=int, default=0)
-    ap.add_argument("--placement", default="", choices=["", "global", "lu-smem", "all-smem", "lu-tmem"],
+    ap.add_argument("--placement", default="", choices=sorted(PLACEMENTS),
                     help="working-set placement (sets the launch shape by hand: no autotuning)")
     ap.add_argument("--accuracy-cells", type=int, default=8192)
     ap.add_argument("--weights", default="", help="seeding network stored by --save-weights (skip training)")
@@ -283,7 +285,7 @@ def solver_kernel_name(tuned, args):
     if sched == "coop":
         return "k_rosenbrock_coop%s_g%d (cooperative solver)" % ("x" if args.parity else "", (bs or 256) // 32)
     return "k_rosenbrock (thread-per-cell solver, %s%s)" % (
-        sched, ", LU slots in tensor memory" if place == PLACEMENTS["lu-tmem"] else "")
+        sched, TMEM_NAMES.get(place, ""))
 
 
 def rel_errors(y, ref):
@@ -598,6 +600,8 @@ def main():
         key = "%s-%s" % (args.precision, sched_used)
         if place_used == PLACEMENTS["lu-tmem"]:
             key += "-tmem"
+        elif place_used == PLACEMENTS["lu-tmem-wide"]:
+            key += "-tmemw"
         if key + "-" + wl in tr:  # a capture of this workload family, if there is one
             key = key + "-" + wl
         if key in tr:

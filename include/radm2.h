@@ -82,6 +82,10 @@ typedef struct radm2_opts {
 #define RADM2_PLACE_ALL_SMEM 3 /* LU, rate constants and state in shared memory (32 threads) */
 #define RADM2_PLACE_LU_TMEM 4  /* the 128 most used LU slots in tensor memory, the rest global
                                   (FP64, 128 or 256 threads per block; with parity, 256) */
+#define RADM2_PLACE_LU_TMEM_WIDE 10 /* the 256 most used LU slots in tensor memory, rate constants
+                                       and state in shared memory, the rest global: one CTA of 128
+                                       threads per SM owns all 512 columns (FP64, persistent,
+                                       fast arithmetic) */
 
 typedef struct radm2_ctx radm2_ctx;
 

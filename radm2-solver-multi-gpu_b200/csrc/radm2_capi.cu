@@ -270,7 +270,9 @@ cudaError_t variant_info(radm2_ctx *c, int bs, SolverInfo *info)
 int default_block_threads(const radm2_opts &o)
 {
     if (o.schedule == RADM2_SCHED_COOP) return 256;
-    if (o.placement == RADM2_PLACE_GLOBAL || o.placement == RADM2_PLACE_LU_TMEM) return 128;
+    if (o.placement == RADM2_PLACE_GLOBAL || o.placement == RADM2_PLACE_LU_TMEM ||
+        o.placement == RADM2_PLACE_LU_TMEM_WIDE)
+        return 128;
     if (o.placement == RADM2_PLACE_LU_SMEM && o.precision == RADM2_PREC_FP32LU) return 64;
     return 32;
 }
@@ -496,9 +498,12 @@ int radm2_create(radm2_ctx **out, const radm2_opts *opts)
         return RADM2_E_ARG;
     if (o.refine_sweeps < 0 || o.refine_sweeps > 2) return RADM2_E_ARG;
     if (o.placement != RADM2_PLACE_GLOBAL && o.placement != RADM2_PLACE_LU_SMEM && o.placement != RADM2_PLACE_ALL_SMEM &&
-        o.placement != RADM2_PLACE_LU_TMEM)
+        o.placement != RADM2_PLACE_LU_TMEM && o.placement != RADM2_PLACE_LU_TMEM_WIDE)
         return RADM2_E_ARG;
     if (o.placement == RADM2_PLACE_LU_TMEM && o.precision != RADM2_PREC_FP64) return RADM2_E_ARG;
+    if (o.placement == RADM2_PLACE_LU_TMEM_WIDE &&
+        (o.precision != RADM2_PREC_FP64 || o.schedule != RADM2_SCHED_PERSISTENT || o.parity))
+        return RADM2_E_ARG;
     if (o.parity != 0 && o.parity != 1) return RADM2_E_ARG;
     if (o.cells_per_thread == 0) o.cells_per_thread = 1;
     if (o.cells_per_thread != 1 && o.cells_per_thread != 2) return RADM2_E_ARG;
@@ -1131,6 +1136,8 @@ int radm2_autotune(radm2_ctx *c, double dt, const double *AbsTol, const double *
             RADM2_VARIANTS_FP64X(RADM2_TUNE_CAND)
         } else if (c->o.precision == RADM2_PREC_FP32LU) {
             RADM2_VARIANTS_FP32(RADM2_TUNE_CAND)
+        } else if (sched == RADM2_SCHED_PERSISTENT) {
+            RADM2_VARIANTS_FP64_PERS(RADM2_TUNE_CAND)
         } else {
             RADM2_VARIANTS_FP64(RADM2_TUNE_CAND)
         }

@@ -53,6 +53,9 @@ cudaError_t launch_reduce(int n, const int *status, const int *nacc, const int *
 // registers per thread (65536 / (bs * minb)) for occupancy.
 #define RADM2_VARIANTS_FP64(X) X(32, 0, 1) X(64, 0, 1) X(128, 0, 1) X(256, 0, 1) X(128, 0, 3) X(128, 0, 4) X(32, 1, 1) X(32, 3, 1) \
     X(128, 4, 1) X(256, 4, 1)
+// Persistent schedule only: one 128-thread CTA per SM owning all of its tensor memory
+// (256 LU slots per thread), rate constants and state in shared memory (RADM2_PLACE_LU_TMEM_WIDE).
+#define RADM2_VARIANTS_FP64_PERS(X) RADM2_VARIANTS_FP64(X) X(128, 10, 1)
 #define RADM2_VARIANTS_FP32(X) X(64, 0, 1) X(128, 0, 1) X(256, 0, 1) X(128, 0, 3) X(128, 0, 4) X(32, 1, 1) X(64, 1, 1) X(32, 3, 1)
 // Reference-arithmetic FP64 solver (radm2_opts.parity): global placement only.
 #define RADM2_VARIANTS_FP64X(X) X(32, 0, 1) X(64, 0, 1) X(128, 0, 1) X(256, 0, 1) X(256, 4, 1)
@@ -77,9 +80,10 @@ struct SolverInfo {
 };
 
 // Solver kernels: one launcher per (precision, schedule) file, variant key
-// bs * 64 + min_blocks * 8 + place (place: bit 0 = LU in shared memory, bit 1 = rate
-// constants and state in shared memory, bit 2 = LU slots in tensor memory; min_blocks <= 4).
-inline int variant_key(int bs, int place, int min_blocks) { return bs * 64 + min_blocks * 8 + place; }
+// bs * 256 + min_blocks * 16 + place (place: bit 0 = LU in shared memory, bit 1 = rate
+// constants and state in shared memory, bit 2 = LU slots in tensor memory, bit 3 = the wide
+// tensor-memory map; min_blocks <= 4).
+inline int variant_key(int bs, int place, int min_blocks) { return bs * 256 + min_blocks * 16 + place; }
 cudaError_t launch_solver_fp64_static(const SolveArgs &a, int key, int grid, cudaStream_t st);
 cudaError_t launch_solver_fp64_persistent(const SolveArgs &a, int key, int grid, cudaStream_t st);
 cudaError_t launch_solver_fp32_static(const SolveArgs &a, int key, int grid, cudaStream_t st);

@@ -13,8 +13,9 @@
 //   RCY  rate constants (156) and state Y (59)             FP64
 //   VEC  Fcn0, K1, K2, K3 and a temporary (5 x 59)          FP64, global scratch
 //   LU   the 659 LU slots                                   LUT (double or float)
-// PLACE selects shared memory for LU (bit 0) and RCY (bit 1); what is not in
-// shared memory lives in the global scratch slot of the thread.
+// PLACE selects shared memory for LU (bit 0) and RCY (bit 1), and tensor memory for the
+// most used LU slots (bit 2: 128 slots per thread; bit 3: 256 slots per thread, one
+// 128-thread CTA per SM); what is not on chip lives in the global scratch slot of the thread.
 //
 // Schedules:
 //   static      one thread per cell, cell = global thread index (the plain method)
@@ -28,11 +29,12 @@
 
 #include "radm2_device.cuh"
 #include "gen/radm2_tmem.h"
+#include "gen/radm2_tmem_wide.h"
 
 namespace radm2 {
 
 enum { SCHED_STATIC = 0, SCHED_PERSISTENT = 1 };
-enum { PLACE_GLOBAL = 0, PLACE_LU_SMEM = 1, PLACE_RCY_SMEM = 2, PLACE_LU_TMEM = 4 };
+enum { PLACE_GLOBAL = 0, PLACE_LU_SMEM = 1, PLACE_RCY_SMEM = 2, PLACE_LU_TMEM = 4, PLACE_LU_TMEM_256 = 8 };
 
 constexpr int RCY_WORDS = NREACT + NVAR;  // 215
 constexpr int RCY_RC = 0, RCY_Y = NREACT;
@@ -53,7 +55,7 @@ struct Layout {
     static constexpr bool lu_smem = (PLACE & PLACE_LU_SMEM) != 0;
     static constexpr int vec_off = 0;  // always global
     static constexpr int rcy_off = rcy_smem ? 0 : VEC_WORDS;
-    static constexpr int lu_off = lu_smem ? (rcy_smem ? RCY_WORDS : 0) : VEC_WORDS + RCY_WORDS;
+    static constexpr int lu_off = lu_smem ? (rcy_smem ? RCY_WORDS : 0) : VEC_WORDS + (rcy_smem ? 0 : RCY_WORDS);
     static constexpr int global_words = VEC_WORDS + (rcy_smem ? 0 : RCY_WORDS) + (lu_smem ? 0 : LuWords<LUT>::value);
     static constexpr int smem_words = (rcy_smem ? RCY_WORDS : 0) + (lu_smem ? LuWords<LUT>::value : 0);
 };
@@ -76,7 +78,8 @@ inline int layout_check(int bs)
     bad |= lu_last >= (L::lu_smem ? scap : gcap);
     // regions must not overlap inside one memory
     if (!L::rcy_smem) bad |= L::rcy_off < L::vec_off + VEC_WORDS;
-    if (!L::lu_smem) bad |= L::lu_off < L::rcy_off + RCY_WORDS;
+    if (!L::lu_smem) bad |= L::lu_off < L::vec_off + VEC_WORDS;
+    if (!L::lu_smem && !L::rcy_smem) bad |= L::lu_off < L::rcy_off + RCY_WORDS;
     if (L::lu_smem && L::rcy_smem) bad |= L::lu_off < RCY_WORDS;
     return bad;
 }
@@ -144,8 +147,9 @@ inline int layout_check(int bs)
 // PLACE_LU_TMEM keeps the RADM2_TMEM_SLOTS most accessed LU slots of every thread in tensor
 // memory instead of its global scratch: thread t of warp w owns lane 32 (w % 4) + t of its
 // CTA's allocation and 256 columns of it (the upper half of a 512-column allocation for warps
-// 4-7), a double in two 32-bit columns.  Tensor memory is separate from the L1 / shared
-// memory array, so it adds on-chip storage without shrinking the cache.  Its loads and stores
+// 4-7), a double in two 32-bit columns.  PLACE_LU_TMEM_256 gives one CTA of 128 threads all
+// 512 columns, so each thread holds the 256 most accessed slots.  Tensor memory is separate
+// from the L1 / shared memory array, so it adds on-chip storage without shrinking the cache.  Its loads and stores
 // are warp-collective (.sync.aligned): every lane of the warp executes them together.
 
 // One double from tensor memory.  The thread's earlier stores are completed first (they may
@@ -177,11 +181,12 @@ struct TmemSlot {
 };
 
 // Slot S of the thread's LU: its global (or shared) scratch word, or with TM its
-// tensor-memory columns when the slot is one of the tensor-memory slots.
+// tensor-memory columns when the slot is one of the tensor-memory slots (TM 1: the
+// 128-slot map, TM 2: the 256-slot map, PLACE_LU_TMEM_256).
 template <int TM, int BS, int S, typename LUT>
 __device__ __forceinline__ decltype(auto) lu_slot(LUT *sg, uint32_t tb)
 {
-    constexpr int col = radm2_tmem_col[S];
+    constexpr int col = TM == 2 ? radm2_tmem_wide_col[S] : radm2_tmem_col[S];
     if constexpr (TM != 0 && col >= 0)
         return TmemSlot{tb + (uint32_t)col};
     else
@@ -250,7 +255,12 @@ __device__ RADM2_PHASE int ph_decomp(LUT *sg, uint32_t tb = 0)
         __syncwarp();                                             \
     } else if (sing == 0 && (v) == (LUT)0)                        \
     sing = (k) + 1
-    if constexpr (TM) {  // tensor-memory slots read and written in groups
+    if constexpr (TM == 2) {  // the 256-slot map (reciprocal form only)
+        static_assert(TM != 2 || RADM2_LU_RECIP, "wide tensor-memory fragments are generated in reciprocal form");
+#define TM_BASE tb
+#include "gen/radm2_decomp_rcp_tm_wide.inc"
+#undef TM_BASE
+    } else if constexpr (TM) {  // tensor-memory slots read and written in groups
 #define TM_BASE tb
 #include RADM2_DECOMP_TM_INC
 #undef TM_BASE
@@ -333,7 +343,13 @@ __device__ RADM2_PHASE void ph_stage(int stage, const double *y, const double *r
 #pragma unroll
         for (int i = 0; i < NVAR; i++) x[i] = VW(VEC_K3 + i) + VW(VEC_K2 + i) * hc32;
     }
-    if constexpr (TM) {
+    if constexpr (TM == 2) {
+#define X(i) x[i]
+#define TM_BASE tb
+#include "gen/radm2_solve_rcp_tm_wide.inc"
+#undef TM_BASE
+#undef X
+    } else if constexpr (TM) {
 #define X(i) x[i]
 #define TM_BASE tb
 #include RADM2_SOLVE_TM_INC
@@ -397,12 +413,14 @@ template <int BS, typename LUT, int SCHED, int PLACE, int MINB, int IR = 1, int 
 __global__ void __launch_bounds__(BS, MINB) k_rosenbrock(const SolveArgs a)
 {
     using L = Layout<LUT, PLACE>;
-    constexpr int TM = (PLACE & PLACE_LU_TMEM) != 0;
+    constexpr int TM = (PLACE & PLACE_LU_TMEM_256) ? 2 : (PLACE & PLACE_LU_TMEM) ? 1 : 0;
     static_assert(!TM || (sizeof(LUT) == 8 && (BS == 128 || BS == 256) && (PLACE & PLACE_LU_SMEM) == 0),
                   "tensor-memory LU slots: FP64, 128 or 256 threads per block, LU otherwise in global scratch");
+    static_assert(TM != 2 || (BS == 128 && (PLACE & PLACE_LU_TMEM) == 0), "wide tensor-memory map: 128 threads");
     // Tensor memory: 256 columns per 128 threads (two CTAs of 128 or one of 256 fill an SM's
-    // 512 columns); warp 0 allocates them and gives up the right to allocate more.
-    constexpr uint32_t TCOLS = BS == 256 ? 512u : 256u;
+    // 512 columns), or with the wide map all 512 columns for one CTA of 128 threads; warp 0
+    // allocates them and gives up the right to allocate more.
+    constexpr uint32_t TCOLS = (BS == 256 || TM == 2) ? 512u : 256u;
     uint32_t talloc = 0, tb = 0;  // the allocation, and this thread's first column in it
     if constexpr (TM) {
         __shared__ uint32_t tmem_base;

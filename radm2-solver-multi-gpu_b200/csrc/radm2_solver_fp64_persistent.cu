@@ -3,4 +3,4 @@
 
 #define RADM2_T double
 #define RADM2_S SCHED_PERSISTENT
-RADM2_DEFINE_SOLVER(fp64_persistent, RADM2_VARIANTS_FP64)
+RADM2_DEFINE_SOLVER(fp64_persistent, RADM2_VARIANTS_FP64_PERS)

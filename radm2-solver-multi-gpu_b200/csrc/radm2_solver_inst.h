@@ -39,6 +39,7 @@ cudaError_t info_one(SolverInfo *out)
     if (e != cudaSuccess) return e;
     // tensor-memory LU slots: 256 columns per 128 threads, 512 per SM
     if ((PLACE & PLACE_LU_TMEM) && blocks * (BS / 128) > 2) blocks = 2 / (BS / 128);
+    if ((PLACE & PLACE_LU_TMEM_256) && blocks > 1) blocks = 1;  // all 512 columns per CTA
     out->regs = at.numRegs;
     out->local_bytes = (int)at.localSizeBytes;
     out->blocks_per_sm = blocks;
@@ -66,7 +67,7 @@ int check_one()
 #define RADM2_ARITH 0
 #endif
 
-#define RADM2_KEY(BS_, PL_, MB_) ((BS_) * 64 + (MB_) * 8 + (PL_))  // = variant_key
+#define RADM2_KEY(BS_, PL_, MB_) ((BS_) * 256 + (MB_) * 16 + (PL_))  // = variant_key
 #define RADM2_CASE_LAUNCH(BS_, PL_, MB_) \
     case RADM2_KEY(BS_, PL_, MB_): return launch_one<BS_, RADM2_T, RADM2_S, PL_, MB_, RADM2_IR, RADM2_ARITH>(a, grid, st);
 #define RADM2_CASE_INFO(BS_, PL_, MB_) \

@@ -383,6 +383,8 @@ def emit_cuda(m, out_dir):
     tcol = emit_tmem(crow, diag, icol, nvar, out_dir)
     for recip in (False, True):
         emit_lu_tm(crow, diag, icol, nvar, tcol, out_dir, recip)
+    wcol = emit_tmem(crow, diag, icol, nvar, out_dir, TMEM_WIDE_SLOTS, "_wide")
+    emit_lu_tm(crow, diag, icol, nvar, wcol, out_dir, True, "_wide")
 
     h.append("\n/* Algorithmic flop counts per call, counted from the emitted expressions */\n")
     for k, v in sorted(flops.items()):
@@ -466,6 +468,7 @@ def emit_lu(crow, diag, icol, nvar, out_dir, recip):
 
 
 TMEM_SLOTS = 128  # doubles of tensor memory per thread (256 32-bit columns)
+TMEM_WIDE_SLOTS = 256  # one 128-thread CTA per SM owning all 512 columns
 
 
 def lu_slot_accesses(crow, diag, icol, nvar):
@@ -491,21 +494,23 @@ def lu_slot_accesses(crow, diag, icol, nvar):
     return acc
 
 
-def emit_tmem(crow, diag, icol, nvar, out_dir):
-    """The LU slots a thread keeps in its tensor-memory row: the TMEM_SLOTS most accessed
-    per step attempt (ties by slot index), each a double in two 32-bit columns."""
+def emit_tmem(crow, diag, icol, nvar, out_dir, nslot=TMEM_SLOTS, tag=""):
+    """The LU slots a thread keeps in its tensor-memory row: the nslot most accessed per
+    step attempt (ties by slot index), each a double in two 32-bit columns.  tag "" is the
+    128-slot map (PLACE_LU_TMEM), "_wide" the 256-slot map (PLACE_LU_TMEM_WIDE)."""
     acc = lu_slot_accesses(crow, diag, icol, nvar)
-    hot = sorted(range(len(icol)), key=lambda s: (-acc[s], s))[:TMEM_SLOTS]
+    hot = sorted(range(len(icol)), key=lambda s: (-acc[s], s))[:nslot]
     col = [-1] * len(icol)
     for i, s in enumerate(sorted(hot)):
         col[s] = 2 * i
-    body = [BANNER, "/* Tensor-memory placement of the LU slots (PLACE_LU_TMEM): the %d slots with the\n"
+    up = tag.upper()
+    body = [BANNER, "/* Tensor-memory placement of the LU slots (PLACE_LU_TMEM%s): the %d slots with the\n"
             " * most loads and stores per step attempt (%d of %d), slot s at 32-bit column\n"
-            " * radm2_tmem_col[s] of the thread's row, -1: global scratch. */\n"
-            % (TMEM_SLOTS, sum(acc[s] for s in hot), sum(acc)),
-            "#pragma once\n#define RADM2_TMEM_SLOTS %d\n" % TMEM_SLOTS,
-            "static constexpr short radm2_tmem_col[%d] = {%s};\n" % (len(col), ",".join(map(str, col)))]
-    write(os.path.join(out_dir, "radm2_tmem.h"), body)
+            " * radm2_tmem%s_col[s] of the thread's row, -1: global scratch. */\n"
+            % (up, nslot, sum(acc[s] for s in hot), sum(acc), tag),
+            "#pragma once\n#define RADM2_TMEM%s_SLOTS %d\n" % (up, nslot),
+            "static constexpr short radm2_tmem%s_col[%d] = {%s};\n" % (tag, len(col), ",".join(map(str, col)))]
+    write(os.path.join(out_dir, "radm2_tmem%s.h" % tag), body)
     return col
 
 
@@ -595,7 +600,7 @@ def tm_store(pairs, col, ind):
     return lines
 
 
-def emit_lu_tm(crow, diag, icol, nvar, col, out_dir, recip):
+def emit_lu_tm(crow, diag, icol, nvar, col, out_dir, recip, tag=""):
     """The LU and triangular solves of emit_lu (reciprocal or division form) for the
     tensor-memory placement: the same operations in the same order, with the tensor-memory
     slots of a row (or of a pivot row's U part) read by wide tcgen05 loads with one wait per
@@ -662,7 +667,7 @@ def emit_lu_tm(crow, diag, icol, nvar, col, out_dir, recip):
             body += tm_store(out, col, "  ")
             body.append(wait_st)
         body.append("}\n")
-    write(os.path.join(out_dir, "radm2_decomp%s_tm.inc" % sfx), body)
+    write(os.path.join(out_dir, "radm2_decomp%s_tm%s.inc" % (sfx, tag)), body)
 
     body = [BANNER, "/* Solve (LU) x = b in place on X(i) (mgpu.cu:2873-3090 order, %s)\n"
             " * with tensor-memory slots loaded in groups.  Accessors: G(s), X(i), TM_BASE. */\n"
@@ -692,7 +697,7 @@ def emit_lu_tm(crow, diag, icol, nvar, col, out_dir, recip):
         for sl in range(diag[k] + 1, crow[k + 1]):
             expr = "(%s - %s * X(%d))" % (expr, ref(sl), icol[sl])
         body.append("  X(%d) = %s %s %s;\n}\n" % (k, expr, "*" if recip else "/", ref(diag[k])))
-    write(os.path.join(out_dir, "radm2_solve%s_tm.inc" % sfx), body)
+    write(os.path.join(out_dir, "radm2_solve%s_tm%s.inc" % (sfx, tag)), body)
 
 
 def slot_chain(t):

@@ -16,6 +16,7 @@ import numpy as np
 NVAR, NFIX, NREACT, NPH, NJVS = 59, 2, 156, 28, 659
 PREC_FP64, PREC_FP32LU = 0, 1
 PLACE_GLOBAL, PLACE_LU_SMEM, PLACE_ALL_SMEM, PLACE_LU_TMEM = 0, 1, 3, 4
+PLACE_LU_TMEM_WIDE = 10  # 256 LU slots in tensor memory, rate constants and state in shared memory
 SCHED_STATIC, SCHED_PERSISTENT, SCHED_COOP = 0, 1, 2
 RADM2_OK, RADM2_E_ARG, RADM2_E_CUDA, RADM2_E_NOMEM, RADM2_E_STATE, RADM2_E_NODEV, RADM2_E_TOOBIG = \
     0, -100, -101, -102, -103, -104, -105

@@ -249,7 +249,9 @@ def test_autotune_picks_fastest_and_keeps_results():
         y_before, acc_before = s.get_state(), int(ipar[13])
         s.set_cells(cells)
         table = s.autotune(600.0, atol, rtol, sample_cells=32768)
-        assert len(table) == 26  # 2 cooperative shapes, 2 x 2 two-cells-per-thread, 10 FP64 variants x 2 schedules
+        # 2 cooperative shapes, 2 x 2 two-cells-per-thread, 10 FP64 variants x 2 schedules, and the
+        # persistent-only wide tensor-memory shape
+        assert len(table) == 27
         ran = [t for t in table if t["ms"] > 0]
         assert len(ran) >= 10 and len({t["attempts"] for t in ran}) == 1
         best = min(ran, key=lambda t: t["ms"])

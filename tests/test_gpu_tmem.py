@@ -1,5 +1,6 @@
-"""Tensor-memory LU slots (RADM2_PLACE_LU_TMEM): the thread-per-cell solver with its 128 most
-used LU slots in tensor memory.
+"""Tensor-memory LU slots: the thread-per-cell solver with its 128 most used LU slots in tensor
+memory (RADM2_PLACE_LU_TMEM), or with its 256 most used slots in tensor memory and its rate
+constants and state in shared memory, one 128-thread CTA per SM (RADM2_PLACE_LU_TMEM_WIDE).
 
 The arithmetic is that of the global-scratch kernel of the same block size and schedule, so
 both must take identical steps and agree to rounding (SAME_ARITH).  Lanes without an attempt
@@ -17,7 +18,11 @@ from radm2b200 import inputs
 
 pytestmark = pytest.mark.gpu
 TMEM = radm2b200.lib.PLACE_LU_TMEM
+WIDE = radm2b200.lib.PLACE_LU_TMEM_WIDE
+PERS = radm2b200.SCHED_PERSISTENT
 PARITY = 1e-10
+# (placement, schedules it is built for)
+PLACES = [(TMEM, (radm2b200.SCHED_STATIC, PERS)), (WIDE, (PERS,))]
 
 
 def run(cells, hstart=6.0, max_steps=0, **opts):
@@ -49,13 +54,28 @@ def test_tmem_equals_global_scratch(mixed4k, schedule, bs):
     assert list(ipar[10:17]) == list(ipar0[10:17])
 
 
+def test_tmem_wide_equals_global_scratch(mixed4k):
+    """The 256-slot map with rate constants and state in shared memory: the same arithmetic
+    as the global-scratch kernel of the same shape, identical steps."""
+    ierr0, y0, st0, _, ipar0 = run(mixed4k, schedule=PERS, block_threads=128)
+    ierr, y, st, _, ipar = run(mixed4k, schedule=PERS, placement=WIDE)
+    assert ierr == ierr0 == 1
+    assert np.array_equal(st["nacc"], st0["nacc"]) and np.array_equal(st["nrej"], st0["nrej"])
+    assert (st["status"] == 1).all()
+    e = rel_err(y, y0).max()
+    print("wide tensor-memory map vs global scratch: max %.2e" % e)
+    assert e <= SAME_ARITH
+    assert list(ipar[10:17]) == list(ipar0[10:17])
+
+
+@pytest.mark.parametrize("place,schedules", PLACES)
 @pytest.mark.parametrize("n", [1, 31, 33, 100, 300])
-def test_tmem_ragged_batches_match_oracle(n):
+def test_tmem_ragged_batches_match_oracle(n, place, schedules):
     """Warps with idle lanes (fewer cells than lanes, ragged last warps): within the fast
     solver's bar of the oracle, identical step counts."""
     cells = inputs.make_cells(n, 29, "plain", 0.3)
-    for schedule in (radm2b200.SCHED_STATIC, radm2b200.SCHED_PERSISTENT):
-        ierr, y, st, rc, _ = run(cells, schedule=schedule, placement=TMEM)
+    for schedule in schedules:
+        ierr, y, st, rc, _ = run(cells, schedule=schedule, placement=place)
         assert ierr == 1 and (st["status"] == 1).all()
         ipar, rpar = radm2b200.default_params(hstart=6.0)
         ok, p = oracle.params(0.0, 600.0, ATOL, RTOL, rpar, ipar)
@@ -64,18 +84,19 @@ def test_tmem_ragged_batches_match_oracle(n):
         assert rel_err(y, y_o).max() <= PARITY
 
 
-def test_tmem_step_cap_and_nonfinite_cell():
+@pytest.mark.parametrize("place", [TMEM, WIDE])
+def test_tmem_step_cap_and_nonfinite_cell(place):
     """Lanes that stop (step cap, a non-finite cell) keep running the collective phases on
     their own scratch; the other cells finish exactly as on the global-scratch kernel."""
     cells = inputs.make_cells(512, 0, "plain")
-    ierr, y, st, _, _ = run(cells, max_steps=5, schedule=radm2b200.SCHED_PERSISTENT, placement=TMEM)
+    ierr, y, st, _, _ = run(cells, max_steps=5, schedule=radm2b200.SCHED_PERSISTENT, placement=place)
     assert ierr == -6 and (st["status"] == -6).all()
     _, y0, _, _, _ = run(cells, max_steps=5, schedule=radm2b200.SCHED_PERSISTENT, block_threads=128)
     assert rel_err(y, y0).max() <= SAME_ARITH
     sub = {k: v[:256].copy() for k, v in cells.items()}
     sub["VAR"][5, 45] = np.nan
     sub["VAR"][200, 3] = np.inf
-    ierr, y, st, _, _ = run(sub, max_steps=300, schedule=radm2b200.SCHED_PERSISTENT, placement=TMEM)
+    ierr, y, st, _, _ = run(sub, max_steps=300, schedule=radm2b200.SCHED_PERSISTENT, placement=place)
     _, y0, st0, _, _ = run(sub, max_steps=300, schedule=radm2b200.SCHED_PERSISTENT, block_threads=128)
     # each cell ends as on the global-scratch kernel (the NaN cell fails; an infinite
     # background species need not)
@@ -94,7 +115,7 @@ def test_tmem_split_graph_and_host_pipeline():
     the same states as on the global-scratch kernel."""
     cells = inputs.make_cells(20000, 9, "mixed")
     outs = []
-    for place in (radm2b200.lib.PLACE_GLOBAL, TMEM):
+    for place in (radm2b200.lib.PLACE_GLOBAL, TMEM, WIDE):
         with radm2b200.Solver(schedule=radm2b200.SCHED_PERSISTENT, block_threads=128, placement=place) as s:
             s.set_cells(cells)
             ipar, rpar = radm2b200.default_params()
@@ -108,8 +129,9 @@ def test_tmem_split_graph_and_host_pipeline():
     # the stiffest cells of this mixed batch amplify the two builds' rounding-level
     # differences (multiply-adds contracted differently): measured 1.1e-13 over two splits
     # and 1.5e-13 for the host call
-    assert rel_err(outs[1][0], outs[0][0]).max() <= 1e-12
-    assert rel_err(outs[1][1], outs[0][1]).max() <= 1e-12
+    for out in outs[1:]:
+        assert rel_err(out[0], outs[0][0]).max() <= 1e-12
+        assert rel_err(out[1], outs[0][1]).max() <= 1e-12
 
 
 def test_tmem_reference_arithmetic(mixed4k):
@@ -145,3 +167,12 @@ def test_tmem_options():
             assert s.rosenbrock(0.0, 600.0, ATOL, RTOL, rpar, ipar) == radm2b200.lib.RADM2_E_ARG
     with radm2b200.Solver(placement=TMEM) as s:
         assert s.opts()["block_threads"] in (0, 128) and s.opts()["placement"] == TMEM
+    # the wide map: FP64, persistent, fast arithmetic, 128 threads per block
+    for bad in ({"precision": radm2b200.PREC_FP32LU}, {"schedule": radm2b200.SCHED_STATIC},
+                {"schedule": radm2b200.SCHED_COOP}, {"parity": 1}, {"cells_per_thread": 2}):
+        with pytest.raises(radm2b200.RadmError):
+            radm2b200.Solver(**dict({"placement": WIDE, "schedule": PERS}, **bad))
+    with radm2b200.Solver(placement=WIDE, schedule=PERS, block_threads=256) as s:  # not built
+        s.set_cells(cells)
+        ipar, rpar = radm2b200.default_params()
+        assert s.rosenbrock(0.0, 600.0, ATOL, RTOL, rpar, ipar) == radm2b200.lib.RADM2_E_ARG
