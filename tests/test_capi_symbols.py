@@ -51,3 +51,20 @@ def test_error_codes_match_header():
     assert len(codes) == 7
     for name, val in codes.items():
         assert getattr(rlib, name) == val, name
+
+
+def test_placement_constants_match_header():
+    """RADM2_PLACE_* values agree between the header, the Python binding and the bench's
+    --placement names."""
+    import importlib.util
+    text = open(os.path.join(ROOT, "include", "radm2.h")).read()
+    places = {m.group(1): int(m.group(2)) for m in re.finditer(r"#define RADM2_(PLACE_\w+)\s+(\d+)", text)}
+    assert places == {"PLACE_GLOBAL": 0, "PLACE_LU_SMEM": 1, "PLACE_ALL_SMEM": 3, "PLACE_LU_TMEM": 4,
+                      "PLACE_LU_TMEM_WIDE": 10}
+    for name, val in places.items():
+        assert getattr(rlib, name) == val, name
+    spec = importlib.util.spec_from_file_location("bench_mod", os.path.join(ROOT, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    assert set(bench.PLACEMENTS.values()) == set(places.values())
+    assert set(bench.TMEM_NAMES) == {places["PLACE_LU_TMEM"], places["PLACE_LU_TMEM_WIDE"]}
