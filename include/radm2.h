@@ -84,8 +84,8 @@ typedef struct radm2_opts {
                                   (FP64, 128 or 256 threads per block; with parity, 256) */
 #define RADM2_PLACE_LU_TMEM_WIDE 10 /* the 256 most used LU slots in tensor memory, rate constants
                                        and state in shared memory, the rest global: one CTA of 128
-                                       threads per SM owns all 512 columns (FP64, persistent,
-                                       fast arithmetic) */
+                                       threads per SM owns all 512 columns (FP64, persistent;
+                                       fast or reference arithmetic) */
 
 typedef struct radm2_ctx radm2_ctx;
 

@@ -501,8 +501,7 @@ int radm2_create(radm2_ctx **out, const radm2_opts *opts)
         o.placement != RADM2_PLACE_LU_TMEM && o.placement != RADM2_PLACE_LU_TMEM_WIDE)
         return RADM2_E_ARG;
     if (o.placement == RADM2_PLACE_LU_TMEM && o.precision != RADM2_PREC_FP64) return RADM2_E_ARG;
-    if (o.placement == RADM2_PLACE_LU_TMEM_WIDE &&
-        (o.precision != RADM2_PREC_FP64 || o.schedule != RADM2_SCHED_PERSISTENT || o.parity))
+    if (o.placement == RADM2_PLACE_LU_TMEM_WIDE && (o.precision != RADM2_PREC_FP64 || o.schedule != RADM2_SCHED_PERSISTENT))
         return RADM2_E_ARG;
     if (o.parity != 0 && o.parity != 1) return RADM2_E_ARG;
     if (o.cells_per_thread == 0) o.cells_per_thread = 1;
@@ -510,8 +509,9 @@ int radm2_create(radm2_ctx **out, const radm2_opts *opts)
     if (o.cells_per_thread == 2 && (o.precision != RADM2_PREC_FP64 || o.placement != RADM2_PLACE_GLOBAL ||
                                     o.min_blocks > 1 || o.parity || o.schedule == RADM2_SCHED_COOP))
         return RADM2_E_ARG;
-    if (o.parity && (o.precision != RADM2_PREC_FP64 ||
-                     (o.placement != RADM2_PLACE_GLOBAL && o.placement != RADM2_PLACE_LU_TMEM)))
+    if (o.parity && (o.precision != RADM2_PREC_FP64 || (o.placement != RADM2_PLACE_GLOBAL &&
+                                                         o.placement != RADM2_PLACE_LU_TMEM &&
+                                                         o.placement != RADM2_PLACE_LU_TMEM_WIDE)))
         return RADM2_E_ARG;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= o.device || o.device < 0) return RADM2_E_NODEV;
@@ -1132,7 +1132,9 @@ int radm2_autotune(radm2_ctx *c, double dt, const double *AbsTol, const double *
     }
     for (int sched = RADM2_SCHED_STATIC; sched <= RADM2_SCHED_PERSISTENT; sched++) {
 #define RADM2_TUNE_CAND(BS_, PL_, MB_) cands.push_back({sched, BS_, PL_, MB_, 1});
-        if (c->o.parity) {
+        if (c->o.parity && sched == RADM2_SCHED_PERSISTENT) {
+            RADM2_VARIANTS_FP64X_PERS(RADM2_TUNE_CAND)
+        } else if (c->o.parity) {
             RADM2_VARIANTS_FP64X(RADM2_TUNE_CAND)
         } else if (c->o.precision == RADM2_PREC_FP32LU) {
             RADM2_VARIANTS_FP32(RADM2_TUNE_CAND)

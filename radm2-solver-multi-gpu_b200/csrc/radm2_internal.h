@@ -59,6 +59,7 @@ cudaError_t launch_reduce(int n, const int *status, const int *nacc, const int *
 #define RADM2_VARIANTS_FP32(X) X(64, 0, 1) X(128, 0, 1) X(256, 0, 1) X(128, 0, 3) X(128, 0, 4) X(32, 1, 1) X(64, 1, 1) X(32, 3, 1)
 // Reference-arithmetic FP64 solver (radm2_opts.parity): global placement only.
 #define RADM2_VARIANTS_FP64X(X) X(32, 0, 1) X(64, 0, 1) X(128, 0, 1) X(256, 0, 1) X(256, 4, 1)
+#define RADM2_VARIANTS_FP64X_PERS(X) RADM2_VARIANTS_FP64X(X) X(128, 10, 1)
 
 // Cooperative kernels (radm2_coop.cuh): 32 cells per block, G roles (warps) per block,
 // one block per SM; the "x" kernel keeps the reference's arithmetic.

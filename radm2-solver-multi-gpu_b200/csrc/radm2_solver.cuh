@@ -94,12 +94,16 @@ inline int layout_check(int bs)
 #if RADM2_LU_RECIP
 #define RADM2_DECOMP_TM_INC "gen/radm2_decomp_rcp_tm.inc"
 #define RADM2_SOLVE_TM_INC "gen/radm2_solve_rcp_tm.inc"
+#define RADM2_DECOMP_TMW_INC "gen/radm2_decomp_rcp_tm_wide.inc"
+#define RADM2_SOLVE_TMW_INC "gen/radm2_solve_rcp_tm_wide.inc"
 #define RADM2_DECOMP_INC "gen/radm2_decomp_rcp.inc"
 #define RADM2_JACLU_INC "gen/radm2_jaclu_rcp.inc"
 #define RADM2_SOLVE_INC "gen/radm2_solve_rcp.inc"
 #else
 #define RADM2_DECOMP_TM_INC "gen/radm2_decomp_tm.inc"
 #define RADM2_SOLVE_TM_INC "gen/radm2_solve_tm.inc"
+#define RADM2_DECOMP_TMW_INC "gen/radm2_decomp_tm_wide.inc"
+#define RADM2_SOLVE_TMW_INC "gen/radm2_solve_tm_wide.inc"
 #define RADM2_DECOMP_INC "gen/radm2_decomp.inc"
 #define RADM2_JACLU_INC "gen/radm2_jaclu.inc"
 #define RADM2_SOLVE_INC "gen/radm2_solve.inc"
@@ -255,10 +259,9 @@ __device__ RADM2_PHASE int ph_decomp(LUT *sg, uint32_t tb = 0)
         __syncwarp();                                             \
     } else if (sing == 0 && (v) == (LUT)0)                        \
     sing = (k) + 1
-    if constexpr (TM == 2) {  // the 256-slot map (reciprocal form only)
-        static_assert(TM != 2 || RADM2_LU_RECIP, "wide tensor-memory fragments are generated in reciprocal form");
+    if constexpr (TM == 2) {  // the 256-slot map
 #define TM_BASE tb
-#include "gen/radm2_decomp_rcp_tm_wide.inc"
+#include RADM2_DECOMP_TMW_INC
 #undef TM_BASE
     } else if constexpr (TM) {  // tensor-memory slots read and written in groups
 #define TM_BASE tb
@@ -346,7 +349,7 @@ __device__ RADM2_PHASE void ph_stage(int stage, const double *y, const double *r
     if constexpr (TM == 2) {
 #define X(i) x[i]
 #define TM_BASE tb
-#include "gen/radm2_solve_rcp_tm_wide.inc"
+#include RADM2_SOLVE_TMW_INC
 #undef TM_BASE
 #undef X
     } else if constexpr (TM) {

@@ -6,4 +6,4 @@
 
 #define RADM2_T double
 #define RADM2_S SCHED_PERSISTENT
-RADM2_DEFINE_SOLVER(fp64x_persistent, RADM2_VARIANTS_FP64X)
+RADM2_DEFINE_SOLVER(fp64x_persistent, RADM2_VARIANTS_FP64X_PERS)

@@ -384,7 +384,8 @@ def emit_cuda(m, out_dir):
     for recip in (False, True):
         emit_lu_tm(crow, diag, icol, nvar, tcol, out_dir, recip)
     wcol = emit_tmem(crow, diag, icol, nvar, out_dir, TMEM_WIDE_SLOTS, "_wide")
-    emit_lu_tm(crow, diag, icol, nvar, wcol, out_dir, True, "_wide")
+    for recip in (False, True):
+        emit_lu_tm(crow, diag, icol, nvar, wcol, out_dir, recip, "_wide")
 
     h.append("\n/* Algorithmic flop counts per call, counted from the emitted expressions */\n")
     for k, v in sorted(flops.items()):

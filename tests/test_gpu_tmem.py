@@ -134,13 +134,15 @@ def test_tmem_split_graph_and_host_pipeline():
         assert rel_err(out[1], outs[0][1]).max() <= 1e-12
 
 
-def test_tmem_reference_arithmetic(mixed4k):
+@pytest.mark.parametrize("place,bs", [(TMEM, 256), (WIDE, 128)])
+def test_tmem_reference_arithmetic(mixed4k, place, bs):
     """Reference arithmetic (radm2_opts.parity: pivot divisions, no multiply-add contraction)
-    with tensor-memory slots: the division-form fragments give the global-scratch parity
-    kernel's results bit for bit, and the oracle's within 1e-10 with identical step counts."""
-    opts = dict(schedule=radm2b200.SCHED_PERSISTENT, block_threads=256, parity=1)
+    with tensor-memory slots (128 per thread, or 256 with the rate constants and state in
+    shared memory): the division-form fragments give the global-scratch parity kernel's
+    results bit for bit, and the oracle's within 1e-10 with identical step counts."""
+    opts = dict(schedule=radm2b200.SCHED_PERSISTENT, block_threads=bs, parity=1)
     ierr0, y0, st0, rc, _ = run(mixed4k, **opts)
-    ierr, y, st, _, _ = run(mixed4k, placement=TMEM, **opts)
+    ierr, y, st, _, _ = run(mixed4k, placement=place, **opts)
     assert ierr == ierr0 == 1
     assert np.array_equal(y, y0) and np.array_equal(st["nacc"], st0["nacc"])
     ipar, rpar = radm2b200.default_params(hstart=6.0)
@@ -148,7 +150,7 @@ def test_tmem_reference_arithmetic(mixed4k):
     y_o, st_o = oracle.integrate(mixed4k["VAR"], mixed4k["FIX"], rc, p)
     assert np.array_equal(st["nacc"], st_o["nacc"]) and np.array_equal(st["nrej"], st_o["nrej"])
     e = rel_err(y, y_o).max()
-    print("reference arithmetic, tensor-memory LU slots, vs oracle: max %.2e" % e)
+    print("reference arithmetic, tensor-memory LU slots (placement %d), vs oracle: max %.2e" % (place, e))
     assert e <= PARITY
 
 
@@ -167,9 +169,9 @@ def test_tmem_options():
             assert s.rosenbrock(0.0, 600.0, ATOL, RTOL, rpar, ipar) == radm2b200.lib.RADM2_E_ARG
     with radm2b200.Solver(placement=TMEM) as s:
         assert s.opts()["block_threads"] in (0, 128) and s.opts()["placement"] == TMEM
-    # the wide map: FP64, persistent, fast arithmetic, 128 threads per block
+    # the wide map: FP64, persistent, 128 threads per block
     for bad in ({"precision": radm2b200.PREC_FP32LU}, {"schedule": radm2b200.SCHED_STATIC},
-                {"schedule": radm2b200.SCHED_COOP}, {"parity": 1}, {"cells_per_thread": 2}):
+                {"schedule": radm2b200.SCHED_COOP}, {"cells_per_thread": 2}):
         with pytest.raises(radm2b200.RadmError):
             radm2b200.Solver(**dict({"placement": WIDE, "schedule": PERS}, **bad))
     with radm2b200.Solver(placement=WIDE, schedule=PERS, block_threads=256) as s:  # not built

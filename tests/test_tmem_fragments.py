@@ -1,7 +1,7 @@
 """The tensor-memory LU and solve fragments (csrc/gen/radm2_{decomp,solve}{_rcp,}_tm.inc: the
-reciprocal-pivot and the division form for the 128-slot map; radm2_{decomp,solve}_rcp_tm_wide.inc:
-the reciprocal form for the 256-slot map) against the plain ones they stand in for, read as
-text on the CPU.
+reciprocal-pivot and the division form for the 128-slot map; radm2_{decomp,solve}{_rcp,}_tm_wide.inc:
+both forms for the 256-slot map) against the plain ones they stand in for, read as text on
+the CPU.
 
 - Every tcgen05 load and store piece covers exactly its slots' columns (radm2_tmem.h,
   radm2_tmem_wide.h): in slot order, two 32-bit columns per double, starting on a multiple of
@@ -34,8 +34,8 @@ PIECE = re.compile(r"tcgen05\.(ld|st)\.sync\.aligned\.32x32b\.x(\d+)\.b32")
 
 
 # (form, map): reciprocal pivots (the fast solver) or divisions (reference arithmetic), with
-# the 128-slot map; reciprocal pivots with the 256-slot map
-FORMS = [("_rcp", ""), ("", ""), ("_rcp", "_wide")]
+# the 128-slot and with the 256-slot map
+FORMS = [("_rcp", ""), ("", ""), ("_rcp", "_wide"), ("", "_wide")]
 
 
 def test_wide_map_holds_the_most_used_slots():
