@@ -68,3 +68,34 @@ def test_placement_constants_match_header():
     spec.loader.exec_module(bench)
     assert set(bench.PLACEMENTS.values()) == set(places.values())
     assert set(bench.TMEM_NAMES) == {places["PLACE_LU_TMEM"], places["PLACE_LU_TMEM_WIDE"]}
+
+
+def test_option_validation_before_device_lookup():
+    """radm2_create checks its options before it looks for a device: on a machine without a
+    GPU an invalid combination returns RADM2_E_ARG and a valid one RADM2_E_NODEV (with a GPU
+    the valid ones create a context, covered by the GPU tests)."""
+    import torch
+    if torch.cuda.is_available():
+        return
+    lib = radm2b200.load()
+
+    def create(**kw):
+        o = rlib.Opts()
+        lib.radm2_opts_default(ctypes.byref(o))
+        for k, v in kw.items():
+            setattr(o, k, v)
+        h = ctypes.c_void_p()
+        return lib.radm2_create(ctypes.byref(h), ctypes.byref(o))
+
+    wide, pers = rlib.PLACE_LU_TMEM_WIDE, radm2b200.SCHED_PERSISTENT
+    ok = [dict(placement=wide, schedule=pers), dict(placement=wide, schedule=pers, parity=1),
+          dict(placement=rlib.PLACE_LU_TMEM), dict(placement=rlib.PLACE_LU_TMEM, parity=1)]
+    bad = [dict(placement=wide), dict(placement=wide, schedule=radm2b200.SCHED_COOP),
+           dict(placement=wide, schedule=pers, precision=radm2b200.PREC_FP32LU),
+           dict(placement=wide, schedule=pers, cells_per_thread=2), dict(placement=7),
+           dict(placement=rlib.PLACE_LU_TMEM, precision=radm2b200.PREC_FP32LU),
+           dict(parity=1, placement=rlib.PLACE_LU_SMEM)]
+    for kw in ok:
+        assert create(**kw) == rlib.RADM2_E_NODEV, kw
+    for kw in bad:
+        assert create(**kw) == rlib.RADM2_E_ARG, kw
